@@ -1,0 +1,850 @@
+// Solver handle of the euler3d_b200 library: device layout construction, the RK5 run loop with
+// on-device stop control, state exchange in the reference's numbering, and the solver half of
+// the C ABI (include/euler3d_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "euler3d_b200.h"
+#include "stage.cuh"
+
+namespace e3d {
+
+void launch_stage_exact(const StageArgs &a, cudaStream_t s);
+void launch_stage_fast(const StageArgs &a, cudaStream_t s);
+
+constexpr int kReduceThreads = 256;
+
+// ------------------------------------------------------------------------------ small kernels
+
+// Sum of the per-block partials in a fixed order, RMS, and the stop tests of
+// EulerSolver::Run (src/solver/EulerSolver.cpp:96-112).
+__global__ void __launch_bounds__(kReduceThreads) finalize_kernel(const double *__restrict__ partials, int n_part,
+                                                                  double n_domain, double *__restrict__ hist,
+                                                                  Control *ctl) {
+    if (ctl->done) return;
+    __shared__ double sh[kReduceThreads];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n_part; i += kReduceThreads) v += partials[i];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    double rms = sqrt(sh[0] / n_domain);
+    if (ctl->n_rms < ctl->hist_cap) hist[ctl->n_rms] = rms;
+    ctl->n_rms += 1;
+    ctl->last_rms = rms;
+    ctl->minit_valid = 0;
+    ctl->sample_now = 0;
+    if (!isfinite(rms)) {  // the reference would spin to MAX_ITER on a NaN; stop and report it
+        ctl->nonfinite = 1;
+        ctl->done = 1;
+        ctl->stop_reason = E3D_STOP_MAX_ITER;
+        return;
+    }
+    if (rms < ctl->min_res) {
+        ctl->done = 1;
+        ctl->stop_reason = E3D_STOP_RESIDUAL;
+        return;
+    }
+    ctl->it += 1;
+    if (ctl->it % ctl->sampling == 0) {
+        ctl->sample_now = 1;
+    } else if (ctl->it >= ctl->max_iter) {
+        ctl->done = 1;
+        ctl->stop_reason = E3D_STOP_MAX_ITER;
+    }
+}
+
+struct CoeffArgs {
+    int n_wall;
+    const int *__restrict__ cell;       // device cell of each wall face, reference wall order
+    const double *__restrict__ svec;    // 3 per wall face: full face normal
+    const double *__restrict__ center;  // 3 per wall face: face centre
+    const double2 *__restrict__ q;
+    double p_inf, cp_factor, cref, sref, ref[3];
+    int axis[3], sign[3];
+    Control *ctl;
+    int run_mode;                       // 1: sampled inside e3d_solver_run, apply the stop test
+    double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
+};
+
+// AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52): face terms in parallel, summed
+// by one thread in the reference's wall order so the sums are the reference's; then
+// EulerSolver::ConvergenceCriteria and the CL/CD/CM selection (src/solver/EulerSolver.cpp:132-152, :253-279).
+__global__ void __launch_bounds__(kReduceThreads) coeff_kernel(CoeffArgs a) {
+    Control *ctl = a.ctl;
+    if (a.run_mode && (ctl->done || !ctl->sample_now)) return;
+    __shared__ double terms[6][kReduceThreads];
+    double F[3] = {0, 0, 0}, CP[3] = {0, 0, 0};
+    for (int base = 0; base < a.n_wall; base += kReduceThreads) {
+        int i = base + threadIdx.x;
+        if (i < a.n_wall) {
+            double p = a.q[3 * a.cell[i] + 2].x;
+            double cp = a.cp_factor * (p - a.p_inf);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double coeff = a.svec[3 * i + k] * cp * a.cref / a.sref;
+                terms[k][threadIdx.x] = coeff;
+                terms[3 + k][threadIdx.x] = coeff * a.center[3 * i + k];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int n = min(kReduceThreads, a.n_wall - base);
+            for (int j = 0; j < n; j++) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    F[k] += terms[k][j];
+                    CP[k] += terms[3 + k][j];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    double lever[3] = {a.ref[0] - CP[0], a.ref[1] - CP[1], a.ref[2] - CP[2]};
+    double M[3] = {(F[1] * lever[2] - F[2] * lever[1]) / a.cref, (F[2] * lever[0] - F[0] * lever[2]) / a.cref,
+                   (F[0] * lever[1] - F[1] * lever[0]) / a.cref};
+    if (!a.run_mode) {
+        for (int k = 0; k < 3; k++) {
+            a.out[k] = F[k];
+            a.out[3 + k] = M[k];
+        }
+        return;
+    }
+    double cl = F[a.axis[0]] * a.sign[0], cd = F[a.axis[1]] * a.sign[1], cm = M[a.axis[2]] * a.sign[2];
+    double tol = ctl->min_aero;
+    bool ok = fabs(ctl->cl - cl) < tol && fabs(ctl->cd - cd) < tol && fabs(ctl->cm - cm) < tol;
+    ctl->counter = ok ? ctl->counter + 1 : 0;
+    ctl->cl = cl;
+    ctl->cd = cd;
+    ctl->cm = cm;
+    for (int k = 0; k < 3; k++) {
+        ctl->force[k] = F[k];
+        ctl->moment[k] = M[k];
+    }
+    if (ctl->counter >= 2) {
+        ctl->done = 1;
+        ctl->stop_reason = E3D_STOP_COEFFICIENTS;
+    } else if (ctl->it >= ctl->max_iter) {
+        ctl->done = 1;
+        ctl->stop_reason = E3D_STOP_MAX_ITER;
+    }
+}
+
+// Reference-ordered FlowField arrays (staging, 8 x T) -> device layout.
+__global__ void load_state_kernel(const double *__restrict__ st, int64_t T, int n_cells, int n_ghosts,
+                                  const int *__restrict__ new2old, const int *__restrict__ ghost_ref,
+                                  double2 *__restrict__ q, double *__restrict__ w0, double *__restrict__ ecell,
+                                  double *__restrict__ minit, double *__restrict__ ghost) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)n_cells;
+    if (i < n_cells) {
+        int o = new2old[i];
+        double rho = st[o], u = st[T + o], v = st[2 * T + o], w = st[3 * T + o];
+        double p = st[4 * T + o], E = st[5 * T + o], H = st[6 * T + o], M = st[7 * T + o];
+        store_prim(q, i, Prim{rho, u, v, w, p, H});
+        w0[0 * N + i] = rho;  // W0 as RungeKutta forms it (src/solver/EulerSolver.cpp:431-438)
+        w0[1 * N + i] = u * rho;
+        w0[2 * N + i] = v * rho;
+        w0[3 * N + i] = w * rho;
+        w0[4 * N + i] = E * rho;
+        ecell[i] = E;
+        minit[i] = M;
+    } else if (i < n_cells + n_ghosts) {
+        int g = i - n_cells;
+        int r = ghost_ref[g];
+        for (int k = 0; k < 8; k++) ghost[8 * (size_t)g + k] = st[k * T + r];
+    }
+}
+
+// Device layout -> reference-ordered FlowField arrays (staging, 8 x T).  Interior Mach is
+// FlowField's c/|u| (src/solver/FlowField.cpp:157) unless the loaded Mach still holds.
+__global__ void store_state_kernel(double *__restrict__ st, int64_t T, int n_cells, int n_ghosts,
+                                   const int *__restrict__ new2old, const int *__restrict__ ghost_ref,
+                                   const double2 *__restrict__ q, const double *__restrict__ ecell,
+                                   const double *__restrict__ minit, const double *__restrict__ ghost, double gamma,
+                                   const Control *ctl) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_cells) {
+        int o = new2old[i];
+        Prim s = load_prim(q, i);
+        double M = ctl->minit_valid ? minit[i] : __ddiv_rn(__dsqrt_rn(__dmul_rn(gamma, __ddiv_rn(s.p, s.rho))),
+                                                           __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(s.u, s.u),
+                                                                                          __dmul_rn(s.v, s.v)),
+                                                                                __dmul_rn(s.w, s.w))));
+        st[o] = s.rho;
+        st[T + o] = s.u;
+        st[2 * T + o] = s.v;
+        st[3 * T + o] = s.w;
+        st[4 * T + o] = s.p;
+        st[5 * T + o] = ecell[i];
+        st[6 * T + o] = s.H;
+        st[7 * T + o] = M;
+    } else if (i < n_cells + n_ghosts) {
+        int g = i - n_cells;
+        int r = ghost_ref[g];
+        for (int k = 0; k < 8; k++) st[k * T + r] = ghost[8 * (size_t)g + k];
+    }
+}
+
+// ------------------------------------------------------------------------------ host handle
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        if (count) E3D_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void upload(const std::vector<T> &v, cudaStream_t s) {
+        alloc(v.size());
+        if (n) E3D_CUDA(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+// Reverse Cuthill-McKee order of the interior cell graph (each connected component from a
+// minimum-degree start, neighbours visited by increasing degree, whole order reversed).
+static std::vector<int> rcm_order(int n, const std::vector<int> &adj_ptr, const std::vector<int> &adj) {
+    std::vector<int> deg(n), order;
+    order.reserve(n);
+    for (int i = 0; i < n; i++) deg[i] = adj_ptr[i + 1] - adj_ptr[i];
+    std::vector<int> by_deg(n);
+    std::iota(by_deg.begin(), by_deg.end(), 0);
+    std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    std::vector<char> seen(n, 0);
+    std::vector<int> nb;
+    for (int start : by_deg) {
+        if (seen[start]) continue;
+        size_t head = order.size();
+        order.push_back(start);
+        seen[start] = 1;
+        while (head < order.size()) {
+            int v = order[head++];
+            nb.clear();
+            for (int k = adj_ptr[v]; k < adj_ptr[v + 1]; k++)
+                if (!seen[adj[k]]) nb.push_back(adj[k]);
+            std::stable_sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+            for (int x : nb) {
+                seen[x] = 1;
+                order.push_back(x);
+            }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+struct Solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int N = 0, G = 0, F = 0, Fint = 0;
+    e3d_flow_params prm{};
+    Freestream fs{};
+    double cp_factor = 0;
+    int n_wall = 0;
+    int n_blocks = 0;
+
+    std::vector<int> new2old, ghost_ref;  // host copies of the maps
+
+    DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell;
+    DevBuf<int2> cf;
+    DevBuf<double4> fgeo, cgeo;
+    DevBuf<double2> q[2];
+    DevBuf<double> w0, ecell, minit, ghost, partials, staging, wall_svec, wall_center, hist, scratch;
+    Control *ctl = nullptr;        // device
+    Control *ctl_host = nullptr;   // pinned mirror
+    int cur = 0;                   // q buffer holding the current state
+    int hist_cap = 0;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~Solver() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell};
+        for (auto *b : ib) b->release();
+        cf.release();
+        fgeo.release();
+        cgeo.release();
+        q[0].release();
+        q[1].release();
+        DevBuf<double> *db[] = {&w0, &ecell, &minit, &ghost, &partials, &staging, &wall_svec, &wall_center, &hist,
+                                &scratch};
+        for (auto *b : db) b->release();
+        if (ctl) cudaFree(ctl);
+        if (ctl_host) cudaFreeHost(ctl_host);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    int64_t state_size() const { return (int64_t)N + G; }
+
+    StageArgs stage_args(int in_buf, double alpha, int first, int last) {
+        StageArgs a{};
+        a.n_cells = N;
+        a.n_ghosts = G;
+        a.cptr = cptr.p;
+        a.cf = cf.p;
+        a.fgeo = fgeo.p;
+        a.cgeo = cgeo.p;
+        a.qin = q[in_buf].p;
+        a.qout = q[1 - in_buf].p;
+        a.w0 = w0.p;
+        a.ecell = ecell.p;
+        a.minit = minit.p;
+        a.ghost = ghost.p;
+        a.partials = partials.p;
+        a.ctl = ctl;
+        a.fs = fs;
+        a.gamma = prm.gamma;
+        a.cfl = prm.cfl;
+        a.alpha = alpha;
+        a.first_stage = first;
+        a.last_stage = last;
+        a.new2old = new2old_d.p;
+        return a;
+    }
+
+    void launch_stage(const StageArgs &a) {
+        if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream);
+        else launch_stage_fast(a, stream);
+    }
+
+    CoeffArgs coeff_args(int buf, int run_mode, double *out) {
+        CoeffArgs c{};
+        c.n_wall = n_wall;
+        c.cell = wall_cell.p;
+        c.svec = wall_svec.p;
+        c.center = wall_center.p;
+        c.q = q[buf].p;
+        c.p_inf = fs.p;
+        c.cp_factor = cp_factor;
+        c.cref = prm.cref;
+        c.sref = prm.sref;
+        for (int k = 0; k < 3; k++) c.ref[k] = prm.ref_point[k];
+        c.axis[0] = prm.cl_axis;
+        c.axis[1] = prm.cd_axis;
+        c.axis[2] = prm.cm_axis;
+        c.sign[0] = prm.cl_sign;
+        c.sign[1] = prm.cd_sign;
+        c.sign[2] = prm.cm_sign;
+        c.ctl = ctl;
+        c.run_mode = run_mode;
+        c.out = out;
+        return c;
+    }
+
+    // One RK5 iteration (EulerSolver.cpp:84-153) starting from q[in_buf]; returns launches.
+    int enqueue_iteration(int in_buf) {
+        static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+        int b = in_buf;
+        for (int s = 0; s < 5; s++) {
+            launch_stage(stage_args(b, alphas[s], s == 0, s == 4));
+            b = 1 - b;
+        }
+        finalize_kernel<<<1, kReduceThreads, 0, stream>>>(partials.p, n_blocks, (double)N, hist.p, ctl);
+        coeff_kernel<<<1, kReduceThreads, 0, stream>>>(coeff_args(b, 1, nullptr));
+        return 7;
+    }
+
+    void build_graph(int iters) {
+        if (graph && graph_iters == iters) return;
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+        cudaGraph_t g;
+        E3D_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int b = 0;
+        for (int i = 0; i < iters; i++) {
+            enqueue_iteration(b);
+            b = 1 - b;  // five stages flip the buffer once per iteration
+        }
+        cudaError_t cap = cudaStreamEndCapture(stream, &g);
+        E3D_CUDA(cap);
+        cudaError_t inst = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        E3D_CUDA(inst);
+        graph_iters = iters;
+    }
+};
+
+static Solver *as_solver(e3d_solver *s) { return reinterpret_cast<Solver *>(s); }
+
+static void check_desc(const e3d_mesh_desc *d) {
+    if (!d) throw Error(E3D_ERR_INVALID_ARG, "mesh descriptor is NULL");
+    if (d->n_cells <= 0 || d->n_faces <= 0 || d->n_faces_int < 0 || d->n_faces_int > d->n_faces)
+        throw Error(E3D_ERR_INVALID_ARG, "mesh sizes are inconsistent");
+    if (!d->face2cell || !d->face_unit_normal || !d->face_normal || !d->face_area || !d->face_center ||
+        !d->cell_volume || !d->cell2face_ptr || !d->cell2face)
+        throw Error(E3D_ERR_INVALID_ARG, "a mesh descriptor array is NULL");
+    if ((int64_t)d->n_cells + (d->n_faces - d->n_faces_int) >= ((int64_t)1 << (31 - kTagBits)))
+        throw Error(E3D_ERR_INVALID_ARG, "mesh too large for the device index encoding");
+    auto chk_list = [&](int n, const int32_t *g, const int32_t *in, const int32_t *f, const char *what) {
+        if (n < 0 || (n > 0 && (!g || !in || !f))) throw Error(E3D_ERR_INVALID_ARG, std::string(what) + " list is invalid");
+    };
+    chk_list(d->n_wall, d->wall_ghost, d->wall_interior, d->wall_face, "wall");
+    chk_list(d->n_farfield, d->farfield_ghost, d->farfield_interior, d->farfield_face, "farfield");
+    chk_list(d->n_sym, d->sym_ghost, d->sym_interior, d->sym_face, "symmetry");
+}
+
+static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solver *S) {
+    check_desc(d);
+    if (!p) throw Error(E3D_ERR_INVALID_ARG, "flow parameters are NULL");
+    if (p->precision != E3D_PREC_FP64_EXACT && p->precision != E3D_PREC_FP64)
+        throw Error(E3D_ERR_INVALID_ARG, "precision mode not available in this build");
+    if (p->scheme != E3D_SCHEME_ROE) throw Error(E3D_ERR_INVALID_ARG, "flux scheme not available in this build");
+    if (p->ordering != E3D_ORDER_NATIVE && p->ordering != E3D_ORDER_RCM)
+        throw Error(E3D_ERR_INVALID_ARG, "unknown cell ordering");
+    if (!(p->gamma > 1.0) || !(p->cfl > 0.0) || !(p->mach >= 0.0) || !(p->cref != 0.0) || !(p->sref != 0.0))
+        throw Error(E3D_ERR_INVALID_ARG, "flow parameters out of range (gamma > 1, cfl > 0, mach >= 0, cref, sref != 0)");
+    for (int ax : {p->cl_axis, p->cd_axis, p->cm_axis})
+        if (ax < 0 || ax > 2) throw Error(E3D_ERR_INVALID_ARG, "coefficient axis must be 0, 1 or 2");
+
+    int ndev = 0;
+    E3D_CUDA(cudaGetDeviceCount(&ndev));
+    if (p->device < 0 || p->device >= ndev) throw Error(E3D_ERR_CUDA, "CUDA device ordinal out of range");
+    cudaDeviceProp prop;
+    E3D_CUDA(cudaGetDeviceProperties(&prop, p->device));
+    if (prop.major != 10) throw Error(E3D_ERR_CUDA, "this library is built for sm_100a (B200); device is sm_" +
+                                                        std::to_string(prop.major) + std::to_string(prop.minor));
+    E3D_CUDA(cudaSetDevice(p->device));
+    S->device = p->device;
+    S->prm = *p;
+    if (p->stream) {
+        S->stream = (cudaStream_t)p->stream;
+    } else {
+        E3D_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+        S->own_stream = true;
+    }
+    const int N = d->n_cells, F = d->n_faces, Fint = d->n_faces_int, G = F - Fint;
+    S->N = N;
+    S->F = F;
+    S->Fint = Fint;
+    S->G = G;
+
+    // ---- validate connectivity and boundary lists
+    for (int f = 0; f < F; f++) {
+        int L = d->face2cell[2 * f], R = d->face2cell[2 * f + 1];
+        if (L < 0 || L >= N) throw Error(E3D_ERR_INVALID_ARG, "face2cell left index out of range at face " + std::to_string(f));
+        if (f < Fint ? (R < 0 || R >= N || R == L) : (R != N + (f - Fint)))
+            throw Error(E3D_ERR_INVALID_ARG, "face2cell right index is not the reference numbering at face " + std::to_string(f));
+    }
+    std::vector<int8_t> bc(G, TAG_FROZEN);
+    auto mark = [&](int n, const int32_t *gh, const int32_t *in, const int32_t *fc, int tag) {
+        for (int i = 0; i < n; i++) {
+            int f = fc[i];
+            if (f < Fint || f >= F || gh[i] != N + (f - Fint) || in[i] != d->face2cell[2 * f])
+                throw Error(E3D_ERR_INVALID_ARG, "boundary list entry inconsistent with face2cell");
+            if (bc[f - Fint] != TAG_FROZEN) throw Error(E3D_ERR_INVALID_ARG, "boundary face listed twice");
+            bc[f - Fint] = (int8_t)tag;
+        }
+    };
+    mark(d->n_wall, d->wall_ghost, d->wall_interior, d->wall_face, TAG_WALL);
+    mark(d->n_sym, d->sym_ghost, d->sym_interior, d->sym_face, TAG_SYM);
+    mark(d->n_farfield, d->farfield_ghost, d->farfield_interior, d->farfield_face, TAG_FAR);
+    if (d->cell2face_ptr[0] != 0) throw Error(E3D_ERR_INVALID_ARG, "cell2face_ptr[0] must be 0");
+    for (int c = 0; c < N; c++)
+        if (d->cell2face_ptr[c + 1] < d->cell2face_ptr[c]) throw Error(E3D_ERR_INVALID_ARG, "cell2face_ptr decreasing");
+    for (int k = 0; k < d->cell2face_ptr[N]; k++)
+        if (d->cell2face[k] < 0 || d->cell2face[k] >= F) throw Error(E3D_ERR_INVALID_ARG, "cell2face index out of range");
+
+    // ---- cell order
+    std::vector<int> new2old(N), old2new(N);
+    if (p->ordering == E3D_ORDER_RCM) {
+        std::vector<int> aptr(N + 1, 0), adj(2 * (size_t)Fint);
+        for (int f = 0; f < Fint; f++) {
+            aptr[d->face2cell[2 * f] + 1]++;
+            aptr[d->face2cell[2 * f + 1] + 1]++;
+        }
+        for (int c = 0; c < N; c++) aptr[c + 1] += aptr[c];
+        std::vector<int> cur(aptr.begin(), aptr.end() - 1);
+        for (int f = 0; f < Fint; f++) {
+            int L = d->face2cell[2 * f], R = d->face2cell[2 * f + 1];
+            adj[cur[L]++] = R;
+            adj[cur[R]++] = L;
+        }
+        new2old = rcm_order(N, aptr, adj);
+    } else {
+        std::iota(new2old.begin(), new2old.end(), 0);
+    }
+    for (int c = 0; c < N; c++) old2new[new2old[c]] = c;
+
+    // ---- per-cell face lists in ascending reference face id (old cell numbering first)
+    std::vector<int> cnt(N + 1, 0);
+    for (int f = 0; f < F; f++) {
+        cnt[d->face2cell[2 * f] + 1]++;
+        if (f < Fint) cnt[d->face2cell[2 * f + 1] + 1]++;
+    }
+    std::vector<int> optr(N + 1, 0);
+    for (int c = 0; c < N; c++) optr[c + 1] = optr[c] + cnt[c + 1];
+    const int64_t M = optr[N];
+    std::vector<int> lst_face(M), lst_code(M);
+    {
+        std::vector<int> fill(optr.begin(), optr.end() - 1);
+        for (int f = 0; f < F; f++) {
+            int L = d->face2cell[2 * f], R = d->face2cell[2 * f + 1];
+            if (f < Fint) {
+                lst_face[fill[L]] = f;
+                lst_code[fill[L]++] = (old2new[R] << kTagBits) | TAG_LEFT;
+                lst_face[fill[R]] = f;
+                lst_code[fill[R]++] = (old2new[L] << kTagBits) | TAG_RIGHT;
+            } else {
+                lst_face[fill[L]] = f;
+                lst_code[fill[L]++] = bc[f - Fint];  // ghost slot filled in below
+            }
+        }
+    }
+    // ---- device order: cells by new index; faces and ghosts by first use in that order
+    std::vector<int> cptr(N + 1, 0);
+    std::vector<int2> cf(M);
+    std::vector<int> face_slot(F, -1), ghost_slot(G, -1);
+    std::vector<double4> fgeo(F), cgeo(N);
+    std::vector<int> ghost_ref(G);
+    int nf = 0, ng = 0;
+    for (int c = 0; c < N; c++) {
+        int o = new2old[c];
+        cptr[c + 1] = cptr[c] + (optr[o + 1] - optr[o]);
+        for (int k = optr[o], j = cptr[c]; k < optr[o + 1]; k++, j++) {
+            int f = lst_face[k];
+            if (face_slot[f] < 0) {
+                face_slot[f] = nf;
+                fgeo[nf] = make_double4(d->face_unit_normal[3 * (size_t)f], d->face_unit_normal[3 * (size_t)f + 1],
+                                        d->face_unit_normal[3 * (size_t)f + 2], d->face_area[f]);
+                nf++;
+            }
+            int code = lst_code[k];
+            if (f >= Fint) {
+                int g = ng++;
+                ghost_slot[f - Fint] = g;
+                ghost_ref[g] = N + (f - Fint);
+                code = (g << kTagBits) | code;
+            }
+            cf[j] = make_int2(code, face_slot[f]);
+        }
+        // spectral-radius face sums in the reference's element-to-face order (TimeIntegration.cpp:209-215)
+        double sx = 0, sy = 0, sz = 0;
+        for (int k = d->cell2face_ptr[o]; k < d->cell2face_ptr[o + 1]; k++) {
+            const double *Sv = d->face_normal + 3 * (size_t)d->cell2face[k];
+            sx += std::fabs(Sv[0]);
+            sy += std::fabs(Sv[1]);
+            sz += std::fabs(Sv[2]);
+        }
+        cgeo[c] = make_double4(sx, sy, sz, d->cell_volume[o]);
+    }
+    if (nf != F || ng != G) throw Error(E3D_ERR_INVALID_ARG, "faces not reached from any cell");
+
+    // ---- freestream, FlowField::Initialize (src/solver/FlowField.cpp:68-101)
+    const double PI = 3.141592653589793238;
+    Freestream fs;
+    fs.rho = 1.0;
+    fs.p = 1.0;
+    fs.M = p->mach;
+    fs.u = p->mach * std::sqrt(p->gamma) * std::cos(p->aoa_deg * (PI / 180));
+    fs.v = p->mach * std::sqrt(p->gamma) * std::sin(p->aoa_deg * (PI / 180));
+    fs.w = 0.0;
+    fs.E = fs.p / ((p->gamma - 1) * fs.rho) + ((fs.u * fs.u + fs.v * fs.v + fs.w * fs.w) / 2.0);
+    fs.H = fs.E + (fs.p / fs.rho);
+    S->fs = fs;
+    double u2 = fs.u * fs.u + fs.v * fs.v + fs.w * fs.w;
+    S->cp_factor = 1 / (0.5 * fs.rho * u2);  // AeroCoefficients ctor, src/solver/AeroCoefficients.cpp:25
+
+    // ---- wall list for the force coefficients (reference wall order)
+    S->n_wall = d->n_wall;
+    std::vector<int> wcell(d->n_wall);
+    std::vector<double> wsv(3 * (size_t)d->n_wall), wct(3 * (size_t)d->n_wall);
+    for (int i = 0; i < d->n_wall; i++) {
+        wcell[i] = old2new[d->wall_interior[i]];
+        for (int k = 0; k < 3; k++) {
+            wsv[3 * i + k] = d->face_normal[3 * (size_t)d->wall_face[i] + k];
+            wct[3 * i + k] = d->face_center[3 * (size_t)d->wall_face[i] + k];
+        }
+    }
+
+    // ---- upload
+    cudaStream_t s = S->stream;
+    S->cptr.upload(cptr, s);
+    S->cf.upload(cf, s);
+    S->fgeo.upload(fgeo, s);
+    S->cgeo.upload(cgeo, s);
+    S->new2old_d.upload(new2old, s);
+    S->ghost_ref_d.upload(ghost_ref, s);
+    S->wall_cell.upload(wcell, s);
+    S->wall_svec.upload(wsv, s);
+    S->wall_center.upload(wct, s);
+    S->q[0].alloc(3 * (size_t)N);
+    S->q[1].alloc(3 * (size_t)N);
+    S->w0.alloc(5 * (size_t)N);
+    S->ecell.alloc(N);
+    S->minit.alloc(N);
+    S->ghost.alloc(8 * (size_t)std::max(G, 1));
+    S->n_blocks = (N + kStageThreads - 1) / kStageThreads;
+    S->partials.alloc(S->n_blocks);
+    S->staging.alloc(8 * (size_t)S->state_size());
+    S->scratch.alloc(6);
+    E3D_CUDA(cudaMalloc(&S->ctl, sizeof(Control)));
+    E3D_CUDA(cudaHostAlloc(&S->ctl_host, sizeof(Control), cudaHostAllocDefault));
+    E3D_CUDA(cudaMemsetAsync(S->ctl, 0, sizeof(Control), s));
+    E3D_CUDA(cudaEventCreate(&S->ev0));
+    E3D_CUDA(cudaEventCreate(&S->ev1));
+    S->new2old = std::move(new2old);
+    S->ghost_ref = std::move(ghost_ref);
+    E3D_CUDA(cudaStreamSynchronize(s));
+}
+
+static void upload_state(Solver *S, const double *const *arr) {
+    const int64_t T = S->state_size();
+    for (int k = 0; k < 8; k++) {
+        if (!arr[k]) throw Error(E3D_ERR_INVALID_ARG, "state array is NULL");
+        E3D_CUDA(cudaMemcpyAsync(S->staging.p + k * T, arr[k], T * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+    }
+    int threads = 256, blocks = (int)((T + threads - 1) / threads);
+    load_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                         S->ghost_ref_d.p, S->q[0].p, S->w0.p, S->ecell.p,
+                                                         S->minit.p, S->ghost.p);
+    E3D_CUDA(cudaGetLastError());
+    S->cur = 0;
+    Control init{};
+    init.minit_valid = 1;
+    std::memcpy(S->ctl_host, &init, sizeof init);
+    E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
+    E3D_CUDA(cudaStreamSynchronize(S->stream));
+}
+
+static void set_freestream(Solver *S) {
+    const int64_t T = S->state_size();
+    std::vector<double> buf(8 * (size_t)T);
+    const double v[8] = {S->fs.rho, S->fs.u, S->fs.v, S->fs.w, S->fs.p, S->fs.E, S->fs.H, S->fs.M};
+    for (int k = 0; k < 8; k++) std::fill(buf.begin() + k * T, buf.begin() + (k + 1) * T, v[k]);
+    const double *arr[8];
+    for (int k = 0; k < 8; k++) arr[k] = buf.data() + k * T;
+    upload_state(S, arr);
+}
+
+}  // namespace e3d
+
+using namespace e3d;
+
+extern "C" {
+
+e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *params, e3d_solver **out) {
+    if (!out) {
+        set_last_error("output handle pointer is NULL");
+        return E3D_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    std::unique_ptr<Solver> S(new (std::nothrow) Solver());
+    if (!S) {
+        set_last_error("host allocation failed");
+        return E3D_ERR_OOM;
+    }
+    e3d_status st = guarded([&] {
+        create_solver(mesh, params, S.get());
+        set_freestream(S.get());
+    });
+    if (st == E3D_OK) *out = reinterpret_cast<e3d_solver *>(S.release());
+    return st;
+}
+
+void e3d_solver_destroy(e3d_solver *solver) {
+    if (!solver) return;
+    Solver *S = as_solver(solver);
+    cudaSetDevice(S->device);
+    if (S->stream) cudaStreamSynchronize(S->stream);
+    delete S;
+}
+
+int64_t e3d_solver_state_size(const e3d_solver *solver) {
+    return solver ? reinterpret_cast<const Solver *>(solver)->state_size() : -1;
+}
+
+e3d_status e3d_solver_set_state(e3d_solver *solver, const double *const state[8]) {
+    return guarded([&] {
+        if (!solver || !state) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        upload_state(S, state);
+    });
+}
+
+e3d_status e3d_solver_set_freestream(e3d_solver *solver) {
+    return guarded([&] {
+        if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        set_freestream(S);
+    });
+}
+
+e3d_status e3d_solver_get_state(e3d_solver *solver, double *const state[8]) {
+    return guarded([&] {
+        if (!solver || !state) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        for (int k = 0; k < 8; k++)
+            if (!state[k]) throw Error(E3D_ERR_INVALID_ARG, "state array is NULL");
+        E3D_CUDA(cudaSetDevice(S->device));
+        const int64_t T = S->state_size();
+        int threads = 256, blocks = (int)((T + threads - 1) / threads);
+        store_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                              S->ghost_ref_d.p, S->q[S->cur].p, S->ecell.p,
+                                                              S->minit.p, S->ghost.p, S->prm.gamma, S->ctl);
+        E3D_CUDA(cudaGetLastError());
+        for (int k = 0; k < 8; k++)
+            E3D_CUDA(cudaMemcpyAsync(state[k], S->staging.p + k * T, T * sizeof(double), cudaMemcpyDeviceToHost,
+                                     S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+    });
+}
+
+e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt) {
+    return guarded([&] {
+        if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        const size_t N = (size_t)S->N;
+        if (S->staging.n < 6 * N) throw Error(E3D_ERR_INVALID_ARG, "staging buffer too small");
+        StageArgs a = S->stage_args(S->cur, 0.0, 1, 0);
+        a.residual_only = 1;
+        a.r_out = S->staging.p;
+        a.dt_out = S->staging.p + 5 * N;
+        a.qout = nullptr;
+        S->launch_stage(a);
+        E3D_CUDA(cudaGetLastError());
+        if (residual)
+            E3D_CUDA(cudaMemcpyAsync(residual, S->staging.p, 5 * N * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+        if (dt) E3D_CUDA(cudaMemcpyAsync(dt, S->staging.p + 5 * N, N * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+    });
+}
+
+e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double moment[3]) {
+    return guarded([&] {
+        if (!solver || !force || !moment) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        coeff_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->coeff_args(S->cur, 0, S->scratch.p));
+        E3D_CUDA(cudaGetLastError());
+        double h[6];
+        E3D_CUDA(cudaMemcpyAsync(h, S->scratch.p, sizeof h, cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+        for (int k = 0; k < 3; k++) {
+            force[k] = h[k];
+            moment[k] = h[3 + k];
+        }
+    });
+}
+
+e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_stats *stats) {
+    return guarded([&] {
+        if (!solver || !rp) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
+        e3d_run_stats st{};
+        const int max_iter = std::max(rp->max_iter, 0);
+        // history buffer
+        if (S->hist_cap < max_iter || !S->hist.p) {
+            S->hist.release();
+            S->hist.alloc(std::max(max_iter, 1));
+            S->hist_cap = std::max(max_iter, 1);
+            if (S->graph) {  // the captured finalize kernels hold the old history pointer
+                cudaGraphExecDestroy(S->graph);
+                S->graph = nullptr;
+            }
+        }
+        // control block: a fresh EulerSolver's counters (_nbInteration = 0, _CL = _CD = _CM = 0)
+        Control init{};
+        init.minit_valid = S->ctl_host->minit_valid;
+        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+        init.minit_valid = S->ctl_host->minit_valid;
+        init.max_iter = max_iter;
+        init.sampling = rp->sampling;
+        init.hist_cap = S->hist_cap;
+        init.min_res = rp->min_residual;
+        init.min_aero = rp->min_aerocoeff_error;
+        init.done = max_iter == 0;
+        std::memcpy(S->ctl_host, &init, sizeof init);
+        E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
+        if (S->cur != 0) {
+            E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
+                                     cudaMemcpyDeviceToDevice, S->stream));
+            S->cur = 0;
+        }
+        int every = rp->check_every > 0 ? rp->check_every : 32;
+        every = std::min(every, std::max(max_iter, 1));
+        every += every & 1;  // whole graphs start and end on buffer 0
+        S->build_graph(every);
+        E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
+        int64_t launches = 0;
+        int launched_iters = 0;
+        while (max_iter > 0) {
+            E3D_CUDA(cudaGraphLaunch(S->graph, S->stream));
+            launches += 7LL * every;
+            launched_iters += every;
+            E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+            E3D_CUDA(cudaStreamSynchronize(S->stream));
+            if (S->ctl_host->done) break;
+            if (launched_iters > max_iter + every)
+                throw Error(E3D_ERR_TIMEOUT, "run did not reach its stop condition");
+        }
+        E3D_CUDA(cudaEventRecord(S->ev1, S->stream));
+        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+        float ms = 0.f;
+        E3D_CUDA(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+        const Control &c = *S->ctl_host;
+        S->cur = c.n_rms & 1;
+        st.iterations = c.it;
+        st.stop_reason = c.stop_reason;
+        st.n_rms = c.n_rms;
+        st.last_rms = c.last_rms;
+        st.cl = c.cl;
+        st.cd = c.cd;
+        st.cm = c.cm;
+        for (int k = 0; k < 3; k++) {
+            st.force[k] = c.force[k];
+            st.moment[k] = c.moment[k];
+        }
+        st.device_ms = ms;
+        st.kernel_launches = launches;
+        if (stats) *stats = st;
+        if (c.nonfinite)
+            throw Error(E3D_ERR_NONFINITE, "density residual became NaN/Inf at iteration " + std::to_string(c.it));
+    });
+}
+
+e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count) {
+    return guarded([&] {
+        if (!solver || !count) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        int n = std::min(S->ctl_host->n_rms, S->hist_cap);
+        *count = n;
+        if (out && capacity > 0 && n > 0)
+            E3D_CUDA(cudaMemcpy(out, S->hist.p, std::min(n, capacity) * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+}  // extern "C"

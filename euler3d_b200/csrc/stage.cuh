@@ -1,0 +1,428 @@
+// Device code of one Runge-Kutta stage of the Euler3D explicit solver, templated on the
+// arithmetic policy.  Included by stage_exact.cu (compiled with -fmad=false: every double
+// operation in the reference's order, no contraction) and stage_fast.cu (restructured
+// arithmetic with FMA, one reciprocal per face, rsqrt instead of sqrt + divide).
+//
+// Layout on the device (cells in a locality order chosen on the host):
+//   cptr[N+1], cf[M]  CSR of each cell's faces sorted by the reference face id, so a cell adds
+//                     its face contributions in exactly the order the reference's face loop
+//                     does (src/solver/EulerSolver.cpp:306-358) -> deterministic, no atomics.
+//                     cf.x = (index << 3) | tag, cf.y = face geometry slot.
+//   fgeo[F]           double4 (unit normal x,y,z ; area)
+//   cgeo[N]           double4 (sum|Sx|, sum|Sy|, sum|Sz| over the cell's faces ; volume)
+//   q[2][3N]          double2 x3 per cell: (rho,u) (v,w) (p,H), ping-pong between stages
+//   w0[5N]            conservative state at the start of the RK step (SoA)
+//   ecell[N]          energy E of the last completed RK step (or of the loaded state)
+//   ghost[8G]         ghost cells, 8 doubles each: rho u v w p E H M
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace e3d {
+
+enum : int { TAG_LEFT = 0, TAG_RIGHT = 1, TAG_WALL = 2, TAG_SYM = 3, TAG_FAR = 4, TAG_FROZEN = 5 };
+constexpr int kTagBits = 3;
+constexpr int kStageThreads = 256;
+
+struct Freestream {
+    double rho, u, v, w, p, E, H, M;
+};
+
+// Run control shared by the kernels of e3d_solver_run; lives in device memory.
+struct Control {
+    int done;          // nonzero: every later kernel returns at once
+    int stop_reason;   // E3D_STOP_*
+    int it;            // EulerSolver::_nbInteration
+    int n_rms;         // iterations whose RMS has been computed
+    int counter;       // consecutive stagnated coefficient samples (src/solver/EulerSolver.cpp:142-147)
+    int sample_now;    // this iteration samples the force coefficients
+    int minit_valid;   // interior Mach of the loaded state still holds (no stage has run since)
+    int nonfinite;     // the RMS became NaN/Inf
+    int max_iter, sampling, hist_cap, pad;
+    double min_res, min_aero, last_rms, cl, cd, cm;
+    double force[3], moment[3];
+};
+
+struct StageArgs {
+    int n_cells, n_ghosts;
+    const int *__restrict__ cptr;
+    const int2 *__restrict__ cf;
+    const double4 *__restrict__ fgeo;
+    const double4 *__restrict__ cgeo;
+    const double2 *__restrict__ qin;
+    double2 *__restrict__ qout;
+    double *__restrict__ w0;
+    double *__restrict__ ecell;
+    const double *__restrict__ minit;
+    double *__restrict__ ghost;
+    double *__restrict__ partials;   // per-block sum of R_rho^2 (last stage only)
+    Control *ctl;
+    Freestream fs;
+    double gamma, cfl, alpha;
+    int first_stage;                 // stage 1 of an iteration (may read the loaded interior Mach)
+    int last_stage;                  // stage 5: write W0/E for the next step and the RMS partials
+    int residual_only;               // e3d_solver_residual: write R and dt, leave the state
+    double *__restrict__ r_out;      // [5N] reference order (residual_only)
+    double *__restrict__ dt_out;     // [N]  reference order (residual_only)
+    const int *__restrict__ new2old;
+};
+
+struct Prim {
+    double rho, u, v, w, p, H;
+};
+
+__device__ __forceinline__ Prim load_prim(const double2 *__restrict__ q, int c) {
+    double2 a = q[3 * c], b = q[3 * c + 1], d = q[3 * c + 2];
+    return Prim{a.x, a.y, b.x, b.y, d.x, d.y};
+}
+
+__device__ __forceinline__ void store_prim(double2 *__restrict__ q, int c, const Prim &s) {
+    q[3 * c] = make_double2(s.rho, s.u);
+    q[3 * c + 1] = make_double2(s.v, s.w);
+    q[3 * c + 2] = make_double2(s.p, s.H);
+}
+
+// ------------------------------------------------------------------------------ Roe flux
+// Exact: Solver::Roe (src/solver/ConvectiveFluxesSchemes.cpp:10-165) operation by operation.
+__device__ __forceinline__ void roe_exact(const Prim &L, const Prim &R, double nx, double ny, double nz,
+                                          double g, double F[5]) {
+    double sl = sqrt(L.rho), sr = sqrt(R.rho);
+    double rt = sqrt(L.rho * R.rho);
+    double ut = (L.u * sl + R.u * sr) / (sl + sr);
+    double vt = (L.v * sl + R.v * sr) / (sl + sr);
+    double wt = (L.w * sl + R.w * sr) / (sl + sr);
+    double ht = (L.H * sl + R.H * sr) / (sl + sr);
+    double q2t = ut * ut + vt * vt + wt * wt;
+    double ct = sqrt((g - 1.0) * (ht - q2t / 2));
+    double Vt = ut * nx + vt * ny + wt * nz;
+    double Vl = L.u * nx + L.v * ny + L.w * nz;
+    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    double drho = R.rho - L.rho, du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w, dp = R.p - L.p, dV = Vr - Vl;
+    double cl = sqrt(g * L.p / L.rho);
+    double delta = (1.0 / 15.0) * cl;
+    double lam1 = fabs(Vt - ct);
+    if (!(fabs(Vt - ct) > delta)) lam1 = ((Vt - ct) * (Vt - ct) + delta * delta) / (2.0 * delta);
+    double lam5 = fabs(Vt + ct);
+    if (!(fabs(Vt + ct) > delta)) lam5 = ((Vt + ct) * (Vt + ct) + delta * delta) / (2.0 * delta);
+    double c2x2 = 2.0 * (ct * ct);
+    double s1 = dp - rt * ct * dV, s5 = dp + rt * ct * dV, s2 = drho - dp / (ct * ct), aV = fabs(Vt);
+    double n[3] = {nx, ny, nz};
+    double ulr[3][2] = {{L.u, R.u}, {L.v, R.v}, {L.w, R.w}};
+    double tl[3] = {ut, vt, wt};
+    double dd[3] = {du, dv, dw};
+    // mass
+    {
+        double favg = (R.rho * Vr + L.rho * Vl) * 0.5;
+        double d1 = 1.0 * lam1 * s1 / c2x2;
+        double d234 = (1.0 * s2 + 0.0) * aV;
+        double d5 = 1.0 * lam5 * s5 / c2x2;
+        F[0] = favg - 0.5 * (d1 + d234 + d5);
+    }
+    // momentum
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double fr = R.rho * Vr * ulr[k][1] + R.p * n[k];
+        double fl = L.rho * Vl * ulr[k][0] + L.p * n[k];
+        double d1 = (tl[k] - ct * n[k]) * lam1 * s1 / c2x2;
+        double d234 = (tl[k] * s2 + rt * (dd[k] - dV * n[k])) * aV;
+        double d5 = (tl[k] + ct * n[k]) * lam5 * s5 / c2x2;
+        F[1 + k] = (fr + fl) * 0.5 - 0.5 * (d1 + d234 + d5);
+    }
+    // energy
+    {
+        double fr = R.rho * Vr * R.H, fl = L.rho * Vl * L.H;
+        double d1 = (ht - ct * Vt) * lam1 * s1 / c2x2;
+        double d234 = (q2t * 0.5 * s2 + rt * (ut * du + vt * dv + wt * dw - Vt * dV)) * aV;
+        double d5 = (ht + ct * Vt) * lam5 * s5 / c2x2;
+        F[4] = (fr + fl) * 0.5 - 0.5 * (d1 + d234 + d5);
+    }
+}
+
+// Fast: the same flux rearranged as F = (F_L + F_R - sum_k a_k r_k) / 2 with the wave strengths
+// a_k formed once, Roe weights from one reciprocal, c~ and 1/c~^2 from one rsqrt, and the left
+// sound speed from rsqrt(gamma p rho).  sl, sr = sqrt(rho) and rcl = rsqrt(gamma p_L rho_L) come
+// from the caller (each is computed once per cell where possible).
+__device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl, double sr, double rcl,
+                                         double nx, double ny, double nz, double g, double F[5]) {
+    double inv = 1.0 / (sl + sr);
+    double wl = sl * inv, wr = sr * inv;
+    double ut = L.u * wl + R.u * wr;
+    double vt = L.v * wl + R.v * wr;
+    double wt = L.w * wl + R.w * wr;
+    double ht = L.H * wl + R.H * wr;
+    double rt = sl * sr;
+    double q2t = ut * ut + vt * vt + wt * wt;
+    double c2 = (g - 1.0) * (ht - 0.5 * q2t);
+    double rc = rsqrt(c2);
+    double ct = c2 * rc, ic2 = rc * rc;
+    double Vt = ut * nx + vt * ny + wt * nz;
+    double Vl = L.u * nx + L.v * ny + L.w * nz;
+    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    double drho = R.rho - L.rho, dp = R.p - L.p, dV = Vr - Vl;
+    double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+    // Harten's fix with delta = c_L / 15 (c_L = gamma p_L * rsqrt(gamma p_L rho_L))
+    double gpl = g * L.p;
+    double delta = (1.0 / 15.0) * (gpl * rcl);
+    double lam1 = fabs(Vt - ct), lam5 = fabs(Vt + ct);
+    if (!(lam1 > delta) || !(lam5 > delta)) {
+        double h = 7.5 * (L.rho * rcl);  // 1 / (2 delta)
+        if (!(lam1 > delta)) lam1 = (lam1 * lam1 + delta * delta) * h;
+        if (!(lam5 > delta)) lam5 = (lam5 * lam5 + delta * delta) * h;
+    }
+    double rcdv = rt * ct * dV;
+    double a1 = 0.5 * lam1 * (dp - rcdv) * ic2;
+    double a5 = 0.5 * lam5 * (dp + rcdv) * ic2;
+    double aV = fabs(Vt);
+    double a2 = aV * (drho - dp * ic2);
+    double a3 = aV * rt;
+    double a15 = a1 + a5, d51 = (a5 - a1) * ct, asum = a15 + a2;
+    double mL = L.rho * Vl, mR = R.rho * Vr;
+    F[0] = 0.5 * (mL + mR - asum);
+    F[1] = 0.5 * (mL * L.u + mR * R.u + (L.p + R.p) * nx - (asum * ut + d51 * nx + a3 * (du - dV * nx)));
+    F[2] = 0.5 * (mL * L.v + mR * R.v + (L.p + R.p) * ny - (asum * vt + d51 * ny + a3 * (dv - dV * ny)));
+    F[3] = 0.5 * (mL * L.w + mR * R.w + (L.p + R.p) * nz - (asum * wt + d51 * nz + a3 * (dw - dV * nz)));
+    F[4] = 0.5 * (mL * L.H + mR * R.H -
+                  (a15 * ht + d51 * Vt + a2 * (0.5 * q2t) + a3 * (ut * du + vt * dv + wt * dw - Vt * dV)));
+}
+
+// ------------------------------------------------------------------------------ ghost states
+// Ghost record: rho u v w p E H M.
+__device__ __forceinline__ void ghost_store(double *gp, double rho, double u, double v, double w, double p,
+                                            double E, double H, double M) {
+    double2 *g2 = reinterpret_cast<double2 *>(gp);
+    g2[0] = make_double2(rho, u);
+    g2[1] = make_double2(v, w);
+    g2[2] = make_double2(p, E);
+    g2[3] = make_double2(H, M);
+}
+
+// Tail shared by subsonic farfield, wall and symmetry ghosts (src/solver/PhysicalBC.cpp:62-66).
+__device__ __forceinline__ void ghost_finish(double *gp, double g, double rho, double u, double v, double w,
+                                             double p, double c, Prim &out) {
+    double q2 = u * u + v * v + w * w;
+    double M = sqrt(q2) / c;
+    double E = p / ((g - 1) * rho) + (q2 / 2.0);
+    double H = E + (p / rho);
+    ghost_store(gp, rho, u, v, w, p, E, H, M);
+    out = Prim{rho, u, v, w, p, H};
+}
+
+// BC::Wall / BC::Symmetry (src/solver/PhysicalBC.cpp:124-231): mirrored velocity.
+__device__ __forceinline__ void ghost_mirror(double *gp, double g, const Prim &d, double nx, double ny, double nz,
+                                             Prim &out) {
+    double c = sqrt(g * (d.p / d.rho));
+    double V = d.u * nx + d.v * ny + d.w * nz;
+    double u = d.u - 2 * V * nx;
+    double v = d.v - 2 * V * ny;
+    double w = d.w - 2 * V * nz;
+    ghost_finish(gp, g, d.rho, u, v, w, d.p, c, out);
+}
+
+// Farfield ghost (EulerSolver::updateBC, src/solver/EulerSolver.cpp:205-227): the branch comes
+// from the ghost's previous Mach and normal velocity; d_M / d_E are the interior Mach and energy.
+__device__ __forceinline__ void ghost_farfield(double *gp, double g, const Freestream &fs, const Prim &d,
+                                               double d_M, double d_E, double nx, double ny, double nz,
+                                               Prim &out) {
+    double2 gu = reinterpret_cast<const double2 *>(gp)[0];
+    double2 gv = reinterpret_cast<const double2 *>(gp)[1];
+    double gM = gp[7];
+    double V = gu.y * nx + gv.x * ny + gv.y * nz;
+    if (gM >= 1.0 && V > 0.0) {  // BC::FarfieldSupersonicOutflow, PhysicalBC.cpp:26-40
+        ghost_store(gp, d.rho, d.u, d.v, d.w, d.p, d_E, d.H, d_M);
+        out = d;
+    } else if (gM < 1.0 && V > 0.0) {  // BC::FarfieldSubsonicOutflow, PhysicalBC.cpp:82-121
+        double c = sqrt(g * (d.p / d.rho));
+        double p = fs.p;
+        double rho = d.rho + (p - d.p) / (c * c);
+        double u = d.u + nx * (d.p - p) / (d.rho * c);
+        double v = d.v + ny * (d.p - p) / (d.rho * c);
+        double w = d.w + nz * (d.p - p) / (d.rho * c);
+        ghost_finish(gp, g, rho, u, v, w, p, c, out);
+    } else if (gM >= 1.0 && V <= 0.0) {  // BC::FarfieldSupersonicInflow, PhysicalBC.cpp:11-23
+        ghost_store(gp, fs.rho, fs.u, fs.v, fs.w, fs.p, fs.E, fs.H, fs.M);
+        out = Prim{fs.rho, fs.u, fs.v, fs.w, fs.p, fs.H};
+    } else if (gM < 1.0 && V <= 0.0) {  // BC::FarfieldSubsonicInflow, PhysicalBC.cpp:43-79
+        double c = sqrt(g * (d.p / d.rho));
+        double p = 0.5 * (fs.p + d.p - d.rho * c * ((nx * (fs.u - d.u)) + (ny * (fs.v - d.v)) + (nz * (fs.w - d.w))));
+        double rho = fs.rho + (p - fs.p) / (c * c);
+        double u = fs.u - nx * (fs.p - p) / (d.rho * c);
+        double v = fs.v - ny * (fs.p - p) / (d.rho * c);
+        double w = fs.w - nz * (fs.p - p) / (d.rho * c);
+        ghost_finish(gp, g, rho, u, v, w, p, c, out);
+    } else {  // NaN Mach or velocity: the reference leaves the ghost as it is
+        double2 gph = reinterpret_cast<const double2 *>(gp)[2];
+        out = Prim{gu.x, gu.y, gv.x, gv.y, gph.x, gp[6]};
+    }
+}
+
+// Physical flux of a ghost state with V = u_ghost . n (Solver::Fc, ConvectiveFluxesSchemes.cpp:167-187).
+__device__ __forceinline__ void ghost_flux(const Prim &s, double nx, double ny, double nz, double F[5]) {
+    double V = s.u * nx + s.v * ny + s.w * nz;
+    F[0] = s.rho * V;
+    F[1] = s.rho * s.u * V + s.p * nx;
+    F[2] = s.rho * s.v * V + s.p * ny;
+    F[3] = s.rho * s.w * V + s.p * nz;
+    F[4] = s.rho * s.H * V;
+}
+
+// ------------------------------------------------------------------------------ the stage
+template <bool EXACT>
+__device__ __forceinline__ void block_sum_store(double v, double *dst) {
+    __shared__ double warp_sums[kStageThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < kStageThreads / 32 ? warp_sums[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) *dst = v;
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads) stage_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    const int c = blockIdx.x * kStageThreads + threadIdx.x;
+    const double g = a.gamma;
+    double r2 = 0.0;
+    if (c < a.n_cells) {
+        const Prim me = load_prim(a.qin, c);
+        // sqrt(rho) and rsqrt(gamma p rho) of this cell, shared by all its faces (fast path)
+        double s_me = 0.0, r_me = 0.0;
+        if (!EXACT) {
+            s_me = sqrt(me.rho);
+            r_me = rsqrt(g * me.p * me.rho);
+        }
+        double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        const int e0 = a.cptr[c], e1 = a.cptr[c + 1];
+        for (int e = e0; e < e1; e++) {
+            const int2 ent = a.cf[e];
+            const int tag = ent.x & ((1 << kTagBits) - 1);
+            const int idx = ent.x >> kTagBits;
+            const double4 fg = a.fgeo[ent.y];
+            double F[5];
+            if (tag <= TAG_RIGHT) {
+                const Prim nb = load_prim(a.qin, idx);
+                if (EXACT) {
+                    if (tag == TAG_LEFT) roe_exact(me, nb, fg.x, fg.y, fg.z, g, F);
+                    else roe_exact(nb, me, fg.x, fg.y, fg.z, g, F);
+                } else {
+                    double s_nb = sqrt(nb.rho);
+                    if (tag == TAG_LEFT) roe_fast(me, nb, s_me, s_nb, r_me, fg.x, fg.y, fg.z, g, F);
+                    else roe_fast(nb, me, s_nb, s_me, rsqrt(g * nb.p * nb.rho), fg.x, fg.y, fg.z, g, F);
+                }
+                if (tag == TAG_LEFT) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) R[k] += F[k] * fg.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) R[k] -= F[k] * fg.w;
+                }
+                continue;
+            }
+            double *gp = a.ghost + 8 * (size_t)idx;
+            Prim gs;
+            if (tag == TAG_WALL) {  // ghost mirrored; flux is the pressure term only (EulerSolver.cpp:331-339)
+                ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+                F[0] = 0;
+                F[1] = fg.x * gs.p;
+                F[2] = fg.y * gs.p;
+                F[3] = fg.z * gs.p;
+                F[4] = 0;
+            } else if (tag == TAG_SYM) {  // Roe against the mirrored ghost (:343-346)
+                ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+                if (EXACT) roe_exact(me, gs, fg.x, fg.y, fg.z, g, F);
+                else roe_fast(me, gs, s_me, s_me, r_me, fg.x, fg.y, fg.z, g, F);  // mirrored rho == rho_me
+            } else {
+                if (tag == TAG_FAR) {
+                    double q2 = me.u * me.u + me.v * me.v + me.w * me.w;
+                    // Mach as FlowField stores it (c/|u|, FlowField.cpp:157) unless the loaded state's
+                    // still holds; E is exact at stage 1 (ecell), recomputed from H at later stages
+                    double dM = (a.first_stage && a.ctl->minit_valid) ? a.minit[c] : sqrt(g * (me.p / me.rho)) / sqrt(q2);
+                    double dE = a.first_stage ? a.ecell[c] : me.H - me.p / me.rho;
+                    ghost_farfield(gp, g, a.fs, me, dM, dE, fg.x, fg.y, fg.z, gs);
+                } else {  // unclassified boundary: the ghost keeps its (freestream) state
+                    double2 g0 = reinterpret_cast<const double2 *>(gp)[0];
+                    double2 g1 = reinterpret_cast<const double2 *>(gp)[1];
+                    double2 g2 = reinterpret_cast<const double2 *>(gp)[2];
+                    gs = Prim{g0.x, g0.y, g1.x, g1.y, g2.x, gp[6]};
+                }
+                ghost_flux(gs, fg.x, fg.y, fg.z, F);  // (:349-357)
+            }
+#pragma unroll
+            for (int k = 0; k < 5; k++) R[k] += F[k] * fg.w;
+        }
+
+        // local time step, TimeStepMethod2 (src/solver/TimeIntegration.cpp:8-40)
+        const double4 cg = a.cgeo[c];
+        double lam, dt;
+        if (EXACT) {
+            double snd = sqrt(g * me.p / me.rho);
+            double lx = 0.5 * (fabs(me.u) + snd) * cg.x;
+            double ly = 0.5 * (fabs(me.v) + snd) * cg.y;
+            double lz = 0.5 * (fabs(me.w) + snd) * cg.z;
+            lam = lx + ly + lz;
+            dt = a.cfl * cg.w / lam;
+        } else {
+            double snd = g * me.p * r_me;
+            lam = 0.5 * ((fabs(me.u) + snd) * cg.x + (fabs(me.v) + snd) * cg.y + (fabs(me.w) + snd) * cg.z);
+            dt = a.cfl * cg.w / lam;
+        }
+
+        if (a.residual_only) {
+            const int o = a.new2old[c];
+#pragma unroll
+            for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
+            a.dt_out[o] = dt;
+            return;
+        }
+
+        // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
+        const size_t N = (size_t)a.n_cells;
+        double W[5];
+        if (EXACT) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - a.alpha * dt * R[k] / cg.w;
+        } else {
+            double coef = a.alpha * a.cfl / lam;  // alpha dt / V
+#pragma unroll
+            for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - coef * R[k];
+        }
+        Prim s;
+        double E;
+        s.rho = W[0];
+        if (EXACT) {
+            s.u = W[1] / s.rho;
+            s.v = W[2] / s.rho;
+            s.w = W[3] / s.rho;
+            E = W[4] / s.rho;
+            double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+            s.p = (g - 1) * s.rho * (E - q2 / 2.0);
+            s.H = E + (s.p / s.rho);
+        } else {
+            double ir = 1.0 / s.rho;
+            s.u = W[1] * ir;
+            s.v = W[2] * ir;
+            s.w = W[3] * ir;
+            E = W[4] * ir;
+            s.p = (g - 1.0) * (W[4] - 0.5 * (W[1] * s.u + W[2] * s.v + W[3] * s.w));
+            s.H = (W[4] + s.p) * ir;
+        }
+        store_prim(a.qout, c, s);
+        if (a.last_stage) {  // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
+            a.w0[0 * N + c] = s.rho;
+            a.w0[1 * N + c] = s.u * s.rho;
+            a.w0[2 * N + c] = s.v * s.rho;
+            a.w0[3 * N + c] = s.w * s.rho;
+            a.w0[4 * N + c] = E * s.rho;
+            a.ecell[c] = E;
+            r2 = R[0] * R[0];
+        }
+    }
+    if (a.last_stage && !a.residual_only) block_sum_store<EXACT>(r2, a.partials + blockIdx.x);
+}
+
+}  // namespace e3d

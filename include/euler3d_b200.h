@@ -1,0 +1,200 @@
+/*
+ * euler3d_b200.h -- C ABI of the B200 (sm_100a) Euler3D explicit-solver hot path.
+ *
+ * The library replaces, for one GPU, the inside of the reference solver's
+ * EulerSolver::Run() loop: ghost-cell boundary updates, the face flux residual,
+ * the local time step, the 5-stage Runge-Kutta update and the residual / force
+ * reductions.  Plain C types only; every pointer here is a HOST pointer unless a
+ * name says otherwise.  All functions return an e3d_status; on failure
+ * e3d_last_error() holds a message (per calling thread).
+ *
+ * Numbering: every array is in the reference's own cell and face numbering
+ * (cells 0..n_cells-1 interior; the ghost cell of boundary face f is
+ * n_cells + f - n_faces_int; faces 0..n_faces_int-1 interior), so results can
+ * be written straight back into the reference's FlowField.  The device keeps
+ * its own locality-ordered copy internally.
+ *
+ * Threading: a solver handle belongs to one host thread at a time; work is
+ * ordered on the handle's CUDA stream.
+ */
+#ifndef EULER3D_B200_H
+#define EULER3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define E3D_ABI_VERSION 1
+
+typedef enum e3d_status {
+	E3D_OK = 0,
+	E3D_ERR_INVALID_ARG = 1, /* null pointer, inconsistent sizes, bad enum value */
+	E3D_ERR_OOM = 2,         /* host or device allocation failed */
+	E3D_ERR_NONFINITE = 3,   /* the solution developed a NaN/Inf or a non-positive density/pressure */
+	E3D_ERR_TIMEOUT = 4,     /* a bounded wait on the device ran out */
+	E3D_ERR_CUDA = 5,        /* a CUDA call failed, or no usable sm_100 device */
+	E3D_ERR_MESH = 6         /* malformed mesh or mesh file */
+} e3d_status;
+
+/* Flux scheme (the reference's SCHEME= key, src/parser/SimConfig.cpp:127-129). */
+enum { E3D_SCHEME_ROE = 0, E3D_SCHEME_AUSM = 1 };
+
+/* Arithmetic of the hot path.
+ *   FP64_EXACT : double precision in the reference's own operation order, no FMA
+ *                contraction; bit-for-bit equal to the reference for the state,
+ *                residual and time step (reductions differ in summation order only).
+ *   FP64       : double precision with restructured arithmetic (fewer divisions and
+ *                square roots, FMA); agrees with the reference to round-off.
+ *   FP32_FLUX  : fluxes, face states and time step in single precision; conservative
+ *                state, Runge-Kutta accumulation and all reductions in double. */
+enum { E3D_PREC_FP64_EXACT = 0, E3D_PREC_FP64 = 1, E3D_PREC_FP32_FLUX = 2 };
+
+/* Cell ordering used on the device (results are always returned in reference order). */
+enum { E3D_ORDER_NATIVE = 0, E3D_ORDER_RCM = 1 };
+
+/* Why e3d_solver_run stopped (the exits of EulerSolver::Run, src/solver/EulerSolver.cpp:100-152). */
+enum { E3D_STOP_MAX_ITER = 0, E3D_STOP_RESIDUAL = 1, E3D_STOP_COEFFICIENTS = 2 };
+
+/* ------------------------------------------------------------------------------------------
+ * Mesh preparation.  Replaces Mesh<MeshPartition>::solveConnectivity
+ * (include/mesh/Mesh.hpp:36-105, src/connectivity/Connectivity.cpp:5-362), the ghost-cell
+ * classification (include/mesh/Mesh.hpp:471-707) and the Metrics constructor
+ * (src/mesh/Metrics.cpp:9-335).  Same numbering and the same IEEE results as the reference.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct e3d_mesh e3d_mesh;
+
+/* Read an SU2 mesh or single-domain .par partition file (src/parser/SU2MeshParser.cpp:12-240,
+ * src/parser/MeshPartition.cpp:15-112) and prepare it.  cref divides the coordinates
+ * (src/mesh/Metrics.cpp:12-19).  n_threads <= 0 uses all host cores. */
+e3d_status e3d_mesh_read(const char *path, double cref, int32_t n_threads, e3d_mesh **out);
+
+/* Prepare a mesh held in memory.  Volume elements: VTK type (10 tetra, 12 hexa, 13 wedge,
+ * 14 pyramid) and CSR node lists.  Markers: n_markers tags; marker m owns surface faces
+ * marker_ptr[m] .. marker_ptr[m+1]-1, face k has nodes face_nodes[face_ptr[k] .. face_ptr[k+1]-1]. */
+e3d_status e3d_mesh_from_arrays(int32_t n_nodes, const double *xyz, int32_t n_elems, const int32_t *elem_vtk,
+                                const int32_t *elem_ptr, const int32_t *elem_nodes, int32_t n_markers,
+                                const char *const *marker_tags, const int32_t *marker_ptr, const int32_t *face_ptr,
+                                const int32_t *face_nodes, double cref, int32_t n_threads, e3d_mesh **out);
+
+/* Sizes of a prepared mesh. */
+typedef struct e3d_mesh_info {
+	int32_t n_cells, n_faces, n_faces_int, n_nodes;
+	int32_t n_wall, n_farfield, n_sym;
+} e3d_mesh_info;
+e3d_status e3d_mesh_info_get(const e3d_mesh *mesh, e3d_mesh_info *info);
+
+/* Read-only view of one prepared array by name: "face2cell", "cell2face_ptr", "cell2face",
+ * "cell2cell", "face2node_ptr", "face2node", "face_normal", "face_unit_normal", "face_center",
+ * "face_area", "cell_volume", "cell_centroid", "{wall,farfield,sym}_{ghost,interior,face}".
+ * *is_double says whether the data is double (else int32).  Valid until e3d_mesh_destroy. */
+e3d_status e3d_mesh_array(const e3d_mesh *mesh, const char *name, const void **data, int64_t *count,
+                          int32_t *is_double);
+void e3d_mesh_destroy(e3d_mesh *mesh);
+
+/* ------------------------------------------------------------------------------------------
+ * Solver.  The descriptor carries what EulerSolver reads from Mesh and Metrics
+ * (include/solver/EulerSolver.hpp:91-95, :206-210); all pointers are host arrays in the
+ * reference numbering, copied during e3d_solver_create and not retained.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct e3d_mesh_desc {
+	int32_t n_cells;                  /* Mesh::GetnElemTot */
+	int32_t n_faces;                  /* Mesh::GetnFace */
+	int32_t n_faces_int;              /* Mesh::GetnFaceInt */
+	const int32_t *face2cell;         /* [2*n_faces]  Mesh::GetFace2ElementID */
+	const double *face_unit_normal;   /* [3*n_faces]  Metrics::getFaceNormalsUnit */
+	const double *face_normal;        /* [3*n_faces]  Metrics::getFaceNormals */
+	const double *face_area;          /* [n_faces]    Metrics::getFaceSurfaces */
+	const double *face_center;        /* [3*n_faces]  Metrics::getFaceCenters */
+	const double *cell_volume;        /* [n_cells]    Metrics::getCellVolumes */
+	const int32_t *cell2face_ptr;     /* [n_cells+1]  Mesh::GetElement2FaceID */
+	const int32_t *cell2face;
+	int32_t n_wall;                   /* Mesh::GetWallGhostCellsIDs / AdjacentGhostCellIDs / AdjacentFaceIDs */
+	const int32_t *wall_ghost, *wall_interior, *wall_face;
+	int32_t n_farfield;               /* Mesh::GetFarfield... */
+	const int32_t *farfield_ghost, *farfield_interior, *farfield_face;
+	int32_t n_sym;                    /* Mesh::GetSymmetry... */
+	const int32_t *sym_ghost, *sym_interior, *sym_face;
+} e3d_mesh_desc;
+
+/* Fill a descriptor whose pointers refer to a prepared mesh's arrays. */
+e3d_status e3d_mesh_describe(const e3d_mesh *mesh, e3d_mesh_desc *desc);
+
+typedef struct e3d_flow_params {
+	double gamma;                     /* GAMMA= */
+	double mach;                      /* FlowField::getM_inf */
+	double aoa_deg;                   /* AOA= */
+	double cfl;                       /* CFL= */
+	double sref, cref;                /* SREF= CREF= */
+	double ref_point[3];              /* MESH_REF_POINT_{X,Y,Z}= */
+	int32_t cl_axis, cl_sign;         /* SimConfig::getMeshOrientationCL */
+	int32_t cd_axis, cd_sign;         /* SimConfig::getMeshOrientationCD */
+	int32_t cm_axis, cm_sign;         /* SimConfig::getMeshOrientationCM */
+	int32_t scheme;                   /* E3D_SCHEME_* */
+	int32_t precision;                /* E3D_PREC_* */
+	int32_t ordering;                 /* E3D_ORDER_* */
+	int32_t device;                   /* CUDA device ordinal */
+	void *stream;                     /* cudaStream_t to run on, or NULL for a library-owned stream */
+} e3d_flow_params;
+
+typedef struct e3d_solver e3d_solver;
+
+/* Replaces the EulerSolver constructor (src/solver/EulerSolver.cpp:21-58) plus the FlowField
+ * freestream initialisation (src/solver/FlowField.cpp:68-101): uploads the mesh and sets
+ * every cell and ghost to the freestream. */
+e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *params, e3d_solver **out);
+void e3d_solver_destroy(e3d_solver *solver);
+
+/* Number of entries of each state array: n_cells + (n_faces - n_faces_int). */
+int64_t e3d_solver_state_size(const e3d_solver *solver);
+
+/* Flow state in FlowField's layout (include/solver/FlowField.hpp:29-59): the 8 arrays
+ * rho, u, v, w, p, E, H, M, each e3d_solver_state_size() long, interior cells then ghosts. */
+e3d_status e3d_solver_set_state(e3d_solver *solver, const double *const state[8]);
+e3d_status e3d_solver_get_state(e3d_solver *solver, double *const state[8]);
+e3d_status e3d_solver_set_freestream(e3d_solver *solver);
+
+typedef struct e3d_run_params {
+	int32_t max_iter;                 /* MAX_ITER= */
+	int32_t sampling;                 /* SAMPLING= (force coefficients every this many iterations) */
+	double min_residual;              /* MIN_RESIDUAL= (absolute density RMS) */
+	double min_aerocoeff_error;       /* MIN_AEROCOEFF_ERROR= (0 disables the coefficient exit) */
+	int32_t check_every;              /* iterations between host checks of the stop flag (0: 32) */
+} e3d_run_params;
+
+typedef struct e3d_run_stats {
+	int32_t iterations;               /* EulerSolver::_nbInteration at exit */
+	int32_t stop_reason;              /* E3D_STOP_* */
+	int32_t n_rms;                    /* iterations whose RMS was computed (history length) */
+	double last_rms;                  /* density RMS of the last iteration run */
+	double cl, cd, cm;                /* last sampled coefficients (EulerSolver::_CL/_CD/_CM) */
+	double force[3], moment[3];       /* last sampled force / moment coefficient vectors */
+	double device_ms;                 /* device time of the iterations (CUDA events) */
+	int64_t kernel_launches;          /* kernels this call launched */
+} e3d_run_stats;
+
+/* Replaces EulerSolver::Run (src/solver/EulerSolver.cpp:60-167): iterate RK5 steps from the
+ * current device state until MAX_ITER, the residual test or the coefficient test stops it. */
+e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *params, e3d_run_stats *stats);
+
+/* Density RMS of every iteration of the last e3d_solver_run (the residuals.dat column). */
+e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count);
+
+/* One call of EulerSolver::updateBC + computeResidual + updateDeltaTime at the current state
+ * (src/solver/EulerSolver.cpp:201-251, :303-359, :362-367): updates the ghost cells and
+ * returns the residual R [5*n_cells, cell-major] and time step dt [n_cells].  Either output
+ * may be NULL. */
+e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt);
+
+/* AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52) on the current state. */
+e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double moment[3]);
+
+const char *e3d_status_string(e3d_status status);
+const char *e3d_last_error(void);
+int32_t e3d_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EULER3D_B200_H */
