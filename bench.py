@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the Euler3D explicit-solver hot path on B200: RK-stage cell-updates/s.
+
+Workload (default): the large all-tetrahedral roofline mesh -- a 128^3 hexahedral box [0,4]^3
+with a Gaussian floor bump (height 0.1, sigma 0.3), every hexahedron split into 6 tetrahedra
+(12,582,912 cells, 25,264,128 faces), nodes jittered 3% (seed 2), Mach 0.6, AoA 0, Roe, CFL 1.0,
+FP64, RCM cell order on the device.  Synthetic, generated in-process (no dataset).
+
+A step is one RK5 iteration (5 stages over every cell, with ghost updates, local time step,
+update, density-RMS reduction and force sampling).  ``value`` counts 5 x cells x steps per
+second with the state resident in HBM; ``e2e`` is the same metric through the C ABI with host
+buffers: the flow state is copied in from pinned host memory and read back every call.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): independent replicas, no data-path collective; the
+timing is the max over ranks.  ``--impl reference`` times the reference's own CPU solver
+(compiled from its sources into oracle/_ref) on a bounded sample of the same mesh family with
+one process per host core, or the CPU oracle port if that binary is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK-stage cell-updates/s"
+UNIT = "cell-updates/s"
+WORKLOAD = "bump_box_tets 128^3x6 (12,582,912 tets), Mach 0.6, Roe, RK5, CFL 1.0"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="hexahedra per box edge (6 tets each)")
+    ap.add_argument("--precision", choices=["fp64", "fp64_exact"], default="fp64")
+    ap.add_argument("--ordering", choices=["rcm", "native"], default="rcm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
+    """FP64 bytes per cell-stage, each array counted once with ideal gather reuse:
+    160 + 40 f_c (f_c = faces per cell): read W, read U0, write W (3 x 40 B), 1/5 of writing U0
+    (8 B), volume (8 B), sum|S| (24 B); per face 2 x int32 + (nx, ny, nz, S) x 8 B."""
+    fc = n_faces / n_cells
+    return 160.0 + 40.0 * fc
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per stage-kernel launch from the committed ncu summary, scaled to this mesh."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_tets.txt")
+    try:
+        vals = {}
+        for line in open(path):
+            if "=" in line and not line.startswith("#"):
+                k, v = line.split("=", 1)
+                vals[k.strip()] = v.strip()
+        return float(vals["dram_bytes_per_cell"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------------------- ours
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from euler3d_b200 import _lib, meshgen
+    from euler3d_b200.solver import STATE_KEYS, EulerSolver, FlowConfig, Mesh
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    t0 = time.time()
+    raw = meshgen.bump_box_tets(args.n)
+    arrays = Mesh.from_raw(raw).arrays()
+    del raw
+    n_cells, n_faces = int(arrays["n_cells"]), int(arrays["n_faces"])
+    prec = _lib.PREC_FP64 if args.precision == "fp64" else _lib.PREC_FP64_EXACT
+    order = _lib.ORDER_RCM if args.ordering == "rcm" else _lib.ORDER_NATIVE
+    flow = FlowConfig(mach=0.6, aoa=0.0, cfl=1.0, precision=prec, ordering=order, device=local_rank)
+    stream = torch.cuda.Stream(device=local_rank)
+    solver = EulerSolver(arrays, flow, stream=stream.cuda_stream)
+    setup_s = time.time() - t0
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up: same graph chunk as the timed run (the graph is instantiated here, not while timing)
+    solver.run(W, check_every=K)
+
+    # ---- timed region: state resident in HBM
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0.record(stream)
+    stats = solver.run(K, check_every=K)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    assert stats["iterations"] == K, stats
+    value = 5.0 * n_cells * K * world / (ms / 1e3)
+
+    # ---- stage-kernel duration for the roofline (direct launches, event pair per launch)
+    prof = solver.run(max(K // 5, 4), profile_stages=True)
+    stage_ms = prof["stage_ms"] / prof["stage_launches"]
+    bytes_per_cell = algorithmic_bytes_per_cell_stage(n_cells, n_faces)
+    achieved = bytes_per_cell * n_cells / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    tr = profiled_traffic()
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        T = solver.state_size
+        host_in = {k: torch.empty(T, dtype=torch.float64).pin_memory().numpy() for k in STATE_KEYS}
+        host_out = {k: torch.empty(T, dtype=torch.float64).pin_memory().numpy() for k in STATE_KEYS}
+        solver.set_freestream()
+        solver.get_state(host_in)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        solver.set_state(host_in)
+        st2 = solver.run(K, check_every=K)
+        solver.get_state(host_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        assert st2["iterations"] == K
+        nbytes = 8 * T * 8
+        e2e = {"value": 5.0 * n_cells * K * world / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
+               "ms": ems, "note": "set_state (pinned host -> device) + run(K) + get_state (device -> pinned host)"}
+
+    # ---- CPU baseline: the oracle port, one RK5 iteration of the same mesh, one core
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+
+        m = po.Mesh(arrays)
+        fl = po.flow(0.6, 0.0, 1.4, 1.0)
+        s = po.freestream(m, fl)
+        t = time.time()
+        po.run(m, fl, s, 1)
+        dt = time.time() - t
+        cpu = {"value": 5.0 * n_cells / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"1 RK5 iteration of the full {n_cells}-cell mesh ({dt:.1f} s), CPU oracle port, 1 thread"}
+
+    launches = stats["kernel_launches"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": n_cells, "faces": n_faces, "faces_per_cell": n_faces / n_cells,
+                   "precision": args.precision, "ordering": args.ordering,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
+                     "kernel": "stage_kernel<false>", "bytes_per_cell_stage": bytes_per_cell,
+                     "avg_launch_ms": stage_ms},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------------------- reference
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from euler3d_b200 import meshgen
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    n = min(args.n, 24)
+    raw = meshgen.bump_box_tets(n)
+    cells = raw.n_cells
+    K, W = max(args.steps // 5, 2), min(args.warmup, 2)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    procs = max(1, min(cores, 64))
+    with tempfile.TemporaryDirectory(prefix="e3dref") as d:
+        cfg = meshgen.CaseConfig(mach=0.6, aoa=0.0, cfl=1.0, max_iter=K, sampling=1)
+        cfg_path = meshgen.write_case(raw, cfg, d)
+        if po.ref_available():
+            kind = "reference"
+            cmd = [po.REF_DRIVER, "bench", cfg_path, str(W), str(K)]
+            t0 = time.time()
+            ps = [subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, cwd=d)
+                  for _ in range(procs)]
+            outs = [p.communicate()[0] for p in ps]
+            secs = []
+            for o in outs:
+                js = [ln for ln in o.splitlines() if ln.startswith("{")]
+                secs.append(json.loads(js[-1])["seconds"])
+            wall = time.time() - t0
+            tmax = max(secs)
+            value = 5.0 * cells * K * procs / tmax
+            sample = (f"{procs} concurrent single-rank reference solver processes (EulerSolver::Run, "
+                      f"compiled from the reference sources), each {K} RK5 iterations of a {n}^3x6 = {cells}-cell "
+                      f"mesh of the same family; slowest process {tmax:.2f} s (wall incl. setup {wall:.0f} s)")
+        else:
+            kind = "port"
+            from euler3d_b200.solver import Mesh
+
+            arrays = Mesh.from_raw(raw).arrays()
+            m = po.Mesh(arrays)
+            fl = po.flow(0.6, 0.0, 1.4, 1.0)
+            s = po.freestream(m, fl)
+            t = time.time()
+            po.run(m, fl, s, K)
+            tmax = time.time() - t
+            procs = 1
+            value = 5.0 * cells * K / tmax
+            sample = f"CPU oracle port, {K} RK5 iterations of a {cells}-cell mesh, 1 thread"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": tmax * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_cells": cells, "processes": procs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,14 +46,14 @@ class FlowParams(C.Structure):
 
 class RunParams(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("sampling", C.c_int32), ("min_residual", C.c_double),
-                ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32)]
+                ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32)]
 
 
 class RunStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("stop_reason", C.c_int32), ("n_rms", C.c_int32),
                 ("last_rms", C.c_double), ("cl", C.c_double), ("cd", C.c_double), ("cm", C.c_double),
                 ("force", C.c_double * 3), ("moment", C.c_double * 3), ("device_ms", C.c_double),
-                ("kernel_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("stage_ms", C.c_double), ("stage_launches", C.c_int64)]
 
 
 class E3DError(RuntimeError):

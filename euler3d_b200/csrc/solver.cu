@@ -278,11 +278,14 @@ struct Solver {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t prof_ev[10] = {};
 
     ~Solver() {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (auto e : prof_ev)
+            if (e) cudaEventDestroy(e);
         DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell};
         for (auto *b : ib) b->release();
         cf.release();
@@ -792,22 +795,55 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
                                      cudaMemcpyDeviceToDevice, S->stream));
             S->cur = 0;
         }
-        int every = rp->check_every > 0 ? rp->check_every : 32;
-        every = std::min(every, std::max(max_iter, 1));
-        every += every & 1;  // whole graphs start and end on buffer 0
-        S->build_graph(every);
-        E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
         int64_t launches = 0;
-        int launched_iters = 0;
-        while (max_iter > 0) {
-            E3D_CUDA(cudaGraphLaunch(S->graph, S->stream));
-            launches += 7LL * every;
-            launched_iters += every;
-            E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
-            E3D_CUDA(cudaStreamSynchronize(S->stream));
-            if (S->ctl_host->done) break;
-            if (launched_iters > max_iter + every)
-                throw Error(E3D_ERR_TIMEOUT, "run did not reach its stop condition");
+        double stage_ms = 0.0;
+        int64_t stage_launches = 0;
+        if (!rp->profile_stages) {
+            int every = rp->check_every > 0 ? rp->check_every : 32;
+            every += every & 1;  // whole graphs start and end on buffer 0
+            S->build_graph(every);
+            E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
+            int launched_iters = 0;
+            while (max_iter > 0) {
+                E3D_CUDA(cudaGraphLaunch(S->graph, S->stream));
+                launches += 7LL * every;
+                launched_iters += every;
+                E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+                E3D_CUDA(cudaStreamSynchronize(S->stream));
+                if (S->ctl_host->done) break;
+                if (launched_iters > max_iter + every)
+                    throw Error(E3D_ERR_TIMEOUT, "run did not reach its stop condition");
+            }
+        } else {
+            // direct launches, an event pair around every stage kernel
+            static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+            if (!S->prof_ev[0]) {
+                for (auto &e : S->prof_ev) E3D_CUDA(cudaEventCreate(&e));
+            }
+            E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
+            int b = 0;
+            for (int it = 0; it < max_iter; it++) {
+                for (int st_i = 0; st_i < 5; st_i++) {
+                    E3D_CUDA(cudaEventRecord(S->prof_ev[2 * st_i], S->stream));
+                    S->launch_stage(S->stage_args(b, alphas[st_i], st_i == 0, st_i == 4));
+                    E3D_CUDA(cudaEventRecord(S->prof_ev[2 * st_i + 1], S->stream));
+                    b = 1 - b;
+                }
+                finalize_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->partials.p, S->n_blocks, (double)S->N,
+                                                                     S->hist.p, S->ctl);
+                coeff_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
+                E3D_CUDA(cudaGetLastError());
+                launches += 7;
+                E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+                E3D_CUDA(cudaStreamSynchronize(S->stream));
+                for (int st_i = 0; st_i < 5; st_i++) {
+                    float ms = 0.f;
+                    E3D_CUDA(cudaEventElapsedTime(&ms, S->prof_ev[2 * st_i], S->prof_ev[2 * st_i + 1]));
+                    stage_ms += ms;
+                }
+                stage_launches += 5;
+                if (S->ctl_host->done) break;
+            }
         }
         E3D_CUDA(cudaEventRecord(S->ev1, S->stream));
         E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
@@ -829,6 +865,8 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         }
         st.device_ms = ms;
         st.kernel_launches = launches;
+        st.stage_ms = stage_ms;
+        st.stage_launches = stage_launches;
         if (stats) *stats = st;
         if (c.nonfinite)
             throw Error(E3D_ERR_NONFINITE, "density residual became NaN/Inf at iteration " + std::to_string(c.it));

@@ -218,13 +218,14 @@ class EulerSolver:
 
     # ---- hot path
     def run(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
-            check_every: int = 0) -> Dict[str, object]:
-        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every)
+            check_every: int = 0, profile_stages: bool = False) -> Dict[str, object]:
+        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages))
         st = _lib.RunStats()
         status = _lib.load().e3d_solver_run(self._h, C.byref(rp), C.byref(st))
         stats = {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,
                  "last_rms": st.last_rms, "cl": st.cl, "cd": st.cd, "cm": st.cm, "force": list(st.force),
-                 "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches}
+                 "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches,
+                 "stage_ms": st.stage_ms, "stage_launches": st.stage_launches}
         check(status)
         return stats
 

@@ -160,7 +160,10 @@ typedef struct e3d_run_params {
 	int32_t sampling;                 /* SAMPLING= (force coefficients every this many iterations) */
 	double min_residual;              /* MIN_RESIDUAL= (absolute density RMS) */
 	double min_aerocoeff_error;       /* MIN_AEROCOEFF_ERROR= (0 disables the coefficient exit) */
-	int32_t check_every;              /* iterations between host checks of the stop flag (0: 32) */
+	int32_t check_every;              /* iterations per CUDA-graph launch between host checks of the
+	                                     stop flag (0: 32); iterations past a stop are no-ops */
+	int32_t profile_stages;           /* 1: launch directly and time every stage kernel with CUDA
+	                                     events (stats.stage_ms); 0: CUDA graphs */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {
@@ -172,6 +175,8 @@ typedef struct e3d_run_stats {
 	double force[3], moment[3];       /* last sampled force / moment coefficient vectors */
 	double device_ms;                 /* device time of the iterations (CUDA events) */
 	int64_t kernel_launches;          /* kernels this call launched */
+	double stage_ms;                  /* profile_stages: summed duration of the stage kernels */
+	int64_t stage_launches;           /* profile_stages: stage kernels timed */
 } e3d_run_stats;
 
 /* Replaces EulerSolver::Run (src/solver/EulerSolver.cpp:60-167): iterate RK5 steps from the
