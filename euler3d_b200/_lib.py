@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(HERE, "libeuler3d_b200.so")
 E3D_OK, E3D_ERR_INVALID_ARG, E3D_ERR_OOM, E3D_ERR_NONFINITE, E3D_ERR_TIMEOUT, E3D_ERR_CUDA, E3D_ERR_MESH = range(7)
 SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
-ORDER_NATIVE, ORDER_RCM = 0, 1
+ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE = 0, 1, 2, 3
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
@@ -46,7 +47,8 @@ class FlowParams(C.Structure):
 
 class RunParams(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("sampling", C.c_int32), ("min_residual", C.c_double),
-                ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32)]
+                ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32),
+                ("stage_kernel", C.c_int32)]
 
 
 class RunStats(C.Structure):
@@ -54,6 +56,12 @@ class RunStats(C.Structure):
                 ("last_rms", C.c_double), ("cl", C.c_double), ("cd", C.c_double), ("cm", C.c_double),
                 ("force", C.c_double * 3), ("moment", C.c_double * 3), ("device_ms", C.c_double),
                 ("kernel_launches", C.c_int64), ("stage_ms", C.c_double), ("stage_launches", C.c_int64)]
+
+
+class SolverInfo(C.Structure):
+    _fields_ = [("n_cells", C.c_int32), ("n_ghosts", C.c_int32), ("n_faces", C.c_int32),
+                ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 4),
+                ("device_bytes", C.c_int64)]
 
 
 class E3DError(RuntimeError):
@@ -76,6 +84,7 @@ SIGNATURES = {
     "e3d_solver_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(FlowParams), C.POINTER(C.c_void_p)]),
     "e3d_solver_destroy": (None, [C.c_void_p]),
     "e3d_solver_state_size": (C.c_int64, [C.c_void_p]),
+    "e3d_solver_info_get": (C.c_int, [C.c_void_p, C.POINTER(SolverInfo)]),
     "e3d_solver_set_state": (C.c_int, [C.c_void_p, C.POINTER(_dp)]),
     "e3d_solver_get_state": (C.c_int, [C.c_void_p, C.POINTER(_dp)]),
     "e3d_solver_set_freestream": (C.c_int, [C.c_void_p]),

@@ -18,10 +18,14 @@
 
 namespace e3d {
 
-void launch_stage_exact(const StageArgs &a, cudaStream_t s);
-void launch_stage_fast(const StageArgs &a, cudaStream_t s);
+void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant);
+void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
+void prepare_tile_exact(size_t smem_bytes);
+void prepare_tile_fast(size_t smem_bytes);
+constexpr int kStageVariants = 3;  // gather (two register budgets), face tile
 
 constexpr int kReduceThreads = 256;
+constexpr int kCoeffThreads = 512;
 
 // ------------------------------------------------------------------------------ small kernels
 
@@ -77,41 +81,71 @@ struct CoeffArgs {
     int axis[3], sign[3];
     Control *ctl;
     int run_mode;                       // 1: sampled inside e3d_solver_run, apply the stop test
+    int sequential;                     // 1: sum in the reference's wall order (FP64_EXACT)
     double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
 };
 
 // AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52): face terms in parallel, summed
 // by one thread in the reference's wall order so the sums are the reference's; then
 // EulerSolver::ConvergenceCriteria and the CL/CD/CM selection (src/solver/EulerSolver.cpp:132-152, :253-279).
-__global__ void __launch_bounds__(kReduceThreads) coeff_kernel(CoeffArgs a) {
+__global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
     Control *ctl = a.ctl;
     if (a.run_mode && (ctl->done || !ctl->sample_now)) return;
-    __shared__ double terms[6][kReduceThreads];
+    __shared__ double terms[6][kCoeffThreads];
     double F[3] = {0, 0, 0}, CP[3] = {0, 0, 0};
-    for (int base = 0; base < a.n_wall; base += kReduceThreads) {
-        int i = base + threadIdx.x;
-        if (i < a.n_wall) {
+    if (a.sequential) {
+        // the reference's order: one running sum over the wall list
+        for (int base = 0; base < a.n_wall; base += kCoeffThreads) {
+            int i = base + threadIdx.x;
+            if (i < a.n_wall) {
+                double p = a.q[3 * a.cell[i] + 2].x;
+                double cp = a.cp_factor * (p - a.p_inf);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    double coeff = a.svec[3 * i + k] * cp * a.cref / a.sref;
+                    terms[k][threadIdx.x] = coeff;
+                    terms[3 + k][threadIdx.x] = coeff * a.center[3 * i + k];
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int n = min(kCoeffThreads, a.n_wall - base);
+                for (int j = 0; j < n; j++) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        F[k] += terms[k][j];
+                        CP[k] += terms[3 + k][j];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    } else {
+        // fixed-shape tree: strided per-thread sums, then a pairwise tree (deterministic)
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = threadIdx.x; i < a.n_wall; i += kCoeffThreads) {
             double p = a.q[3 * a.cell[i] + 2].x;
             double cp = a.cp_factor * (p - a.p_inf);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 double coeff = a.svec[3 * i + k] * cp * a.cref / a.sref;
-                terms[k][threadIdx.x] = coeff;
-                terms[3 + k][threadIdx.x] = coeff * a.center[3 * i + k];
+                acc[k] += coeff;
+                acc[3 + k] += coeff * a.center[3 * i + k];
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int n = min(kReduceThreads, a.n_wall - base);
-            for (int j = 0; j < n; j++) {
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    F[k] += terms[k][j];
-                    CP[k] += terms[3 + k][j];
-                }
-            }
-        }
+        for (int k = 0; k < 6; k++) terms[k][threadIdx.x] = acc[k];
         __syncthreads();
+        for (int st = kCoeffThreads / 2; st > 0; st >>= 1) {
+            if (threadIdx.x < st)
+#pragma unroll
+                for (int k = 0; k < 6; k++) terms[k][threadIdx.x] += terms[k][threadIdx.x + st];
+            __syncthreads();
+        }
+        for (int k = 0; k < 3; k++) {
+            F[k] = terms[k][0];
+            CP[k] = terms[3 + k][0];
+        }
     }
     if (threadIdx.x != 0) return;
     double lever[3] = {a.ref[0] - CP[0], a.ref[1] - CP[1], a.ref[2] - CP[2]};
@@ -265,7 +299,13 @@ struct Solver {
 
     std::vector<int> new2old, ghost_ref;  // host copies of the maps
 
-    DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell;
+    DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell, tile_halo_ptr, tile_halo, tile_face_ptr;
+    DevBuf<int2> tile_face;
+    DevBuf<unsigned short> tile_contrib;
+    bool tiles_ok = false;
+    int max_contrib = 0, smem_cells = 0, smem_faces = 0;
+    size_t tile_smem = 0;
+    int64_t tile_faces_total = 0;
     DevBuf<int2> cf;
     DevBuf<double4> fgeo, cgeo;
     DevBuf<double2> q[2];
@@ -286,8 +326,10 @@ struct Solver {
         if (ev1) cudaEventDestroy(ev1);
         for (auto e : prof_ev)
             if (e) cudaEventDestroy(e);
-        DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell};
+        DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell, &tile_halo_ptr, &tile_halo, &tile_face_ptr};
         for (auto *b : ib) b->release();
+        tile_face.release();
+        tile_contrib.release();
         cf.release();
         fgeo.release();
         cgeo.release();
@@ -302,6 +344,14 @@ struct Solver {
     }
 
     int64_t state_size() const { return (int64_t)N + G; }
+
+    int64_t device_bytes() const {
+        return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
+                         tile_face_ptr.n) * 4 + (int64_t)(cf.n + tile_face.n) * 8 + (int64_t)tile_contrib.n * 2 +
+               (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
+               (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
+                         hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
+    }
 
     StageArgs stage_args(int in_buf, double alpha, int first, int last) {
         StageArgs a{};
@@ -326,12 +376,61 @@ struct Solver {
         a.first_stage = first;
         a.last_stage = last;
         a.new2old = new2old_d.p;
+        a.tile_halo_ptr = tile_halo_ptr.p;
+        a.tile_halo = tile_halo.p;
+        a.tile_face_ptr = tile_face_ptr.p;
+        a.tile_face = tile_face.p;
+        a.tile_contrib = tile_contrib.p;
+        a.max_contrib = max_contrib;
+        a.smem_cells = smem_cells;
+        a.smem_faces = smem_faces;
+        a.fint_dev = Fint;
         return a;
     }
 
-    void launch_stage(const StageArgs &a) {
-        if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream);
-        else launch_stage_fast(a, stream);
+    int variant = 0;                // stage-kernel variant picked by autotune()
+    float variant_ms[kStageVariants] = {};
+
+    void launch_stage(const StageArgs &a, int v = -1) {
+        if (v < 0) v = variant;
+        if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
+        else launch_stage_fast(a, stream, v);
+    }
+
+    // Time every stage-kernel variant on this mesh and keep the fastest.  The trial launches
+    // read the current state and write only scratch: the other state buffer (overwritten by the
+    // next real stage anyway) and a copy of the ghost cells; W0, E and the RMS partials are
+    // untouched (not a last stage), so results do not depend on the tuning.
+    void autotune() {
+        DevBuf<double> ghost_copy;
+        ghost_copy.alloc(ghost.n);
+        E3D_CUDA(cudaMemcpyAsync(ghost_copy.p, ghost.p, ghost.n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        StageArgs a = stage_args(cur, 0.0533, 1, 0);
+        a.ghost = ghost_copy.p;
+        const int reps = N > 200000 ? 3 : 10;
+        float best = 1e30f;
+        if (tiles_ok) {
+            if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem);
+            else prepare_tile_fast(tile_smem);
+        }
+        for (int v = 0; v < kStageVariants; v++) {
+            variant_ms[v] = -1.0f;
+            if (v == 2 && !tiles_ok) continue;
+            launch_stage(a, v);  // warm
+            E3D_CUDA(cudaEventRecord(ev0, stream));
+            for (int r = 0; r < reps; r++) launch_stage(a, v);
+            E3D_CUDA(cudaEventRecord(ev1, stream));
+            E3D_CUDA(cudaEventSynchronize(ev1));
+            float ms = 0.f;
+            E3D_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            variant_ms[v] = ms / reps;
+            if (variant_ms[v] < best) {
+                best = variant_ms[v];
+                variant = v;
+            }
+        }
+        E3D_CUDA(cudaGetLastError());
+        ghost_copy.release();
     }
 
     CoeffArgs coeff_args(int buf, int run_mode, double *out) {
@@ -354,6 +453,7 @@ struct Solver {
         c.sign[2] = prm.cm_sign;
         c.ctl = ctl;
         c.run_mode = run_mode;
+        c.sequential = prm.precision == E3D_PREC_FP64_EXACT;
         c.out = out;
         return c;
     }
@@ -367,7 +467,7 @@ struct Solver {
             b = 1 - b;
         }
         finalize_kernel<<<1, kReduceThreads, 0, stream>>>(partials.p, n_blocks, (double)N, hist.p, ctl);
-        coeff_kernel<<<1, kReduceThreads, 0, stream>>>(coeff_args(b, 1, nullptr));
+        coeff_kernel<<<1, kCoeffThreads, 0, stream>>>(coeff_args(b, 1, nullptr));
         return 7;
     }
 
@@ -412,13 +512,151 @@ static void check_desc(const e3d_mesh_desc *d) {
     chk_list(d->n_sym, d->sym_ghost, d->sym_interior, d->sym_face, "symmetry");
 }
 
+// Face tiles for tile_kernel.  Tile t owns cells [t*T, t*T + T); its local cells are the owned
+// ones followed by the halo (outside neighbours, ascending); its faces are every interior face with
+// an owned cell (once, interior ones before boundary ones) and its owned cells' boundary faces; each
+// owned cell lists its faces in the order of its gather list (ascending reference face id).  Tiles
+// whose local cells or faces exceed the entry encoding leave the variant disabled.
+static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vector<int2> &cf, int Fint) {
+    const int N = S->N, T = kTileCells;
+    const int n_tiles = (N + T - 1) / T;
+    std::vector<int> halo_ptr(n_tiles + 1, 0), halo, face_ptr(n_tiles + 1, 0);
+    std::vector<int2> tface;
+    int max_contrib = 0;
+    for (int c = 0; c < N; c++) max_contrib = std::max(max_contrib, cptr[c + 1] - cptr[c]);
+    std::vector<unsigned short> contrib((size_t)n_tiles * max_contrib * T, kNoContrib);
+    std::vector<int> face_local(Fint, -1), face_tile(Fint, -1);
+    int max_cells = 0, max_faces = 0;
+    bool ok = max_contrib > 0;
+    std::vector<int> hl, bnd;
+    for (int t = 0; t < n_tiles && ok; t++) {
+        const int c0 = t * T, c1 = std::min(N, c0 + T);
+        hl.clear();
+        for (int c = c0; c < c1; c++)
+            for (int e = cptr[c]; e < cptr[c + 1]; e++) {
+                int tag = cf[e].x & ((1 << kTagBits) - 1);
+                int nb = cf[e].x >> kTagBits;
+                if (tag <= TAG_RIGHT && (nb < c0 || nb >= c1)) hl.push_back(nb);
+            }
+        std::sort(hl.begin(), hl.end());
+        hl.erase(std::unique(hl.begin(), hl.end()), hl.end());
+        auto local = [&](int cell) {
+            if (cell >= c0 && cell < c1) return cell - c0;
+            return (c1 - c0) + (int)(std::lower_bound(hl.begin(), hl.end(), cell) - hl.begin());
+        };
+        const int nloc = (c1 - c0) + (int)hl.size();
+        if (nloc > (1 << kTileLocalBits)) {
+            ok = false;
+            break;
+        }
+        const int fbase = (int)tface.size();
+        bnd.clear();
+        // interior faces first (one entry per face), boundary faces after
+        for (int c = c0; c < c1; c++)
+            for (int e = cptr[c]; e < cptr[c + 1]; e++) {
+                int tag = cf[e].x & ((1 << kTagBits) - 1);
+                int slot = cf[e].y;
+                if (tag > TAG_RIGHT) {
+                    bnd.push_back(e);
+                    continue;
+                }
+                if (face_tile[slot] == t) continue;
+                face_tile[slot] = t;
+                face_local[slot] = (int)tface.size() - fbase;
+                int nb = cf[e].x >> kTagBits;
+                int l = tag == TAG_LEFT ? local(c) : local(nb);
+                int r = tag == TAG_LEFT ? local(nb) : local(c);
+                tface.push_back(make_int2(l | (r << kTileLocalBits) | (TAG_LEFT << (2 * kTileLocalBits)), slot));
+            }
+        std::vector<int> bnd_local(bnd.size());
+        for (size_t b = 0; b < bnd.size(); b++) {
+            int e = bnd[b];
+            int tag = cf[e].x & ((1 << kTagBits) - 1);
+            int c = (int)(std::upper_bound(cptr.begin(), cptr.end(), e) - cptr.begin()) - 1;
+            bnd_local[b] = (int)tface.size() - fbase;
+            tface.push_back(make_int2(local(c) | (tag << (2 * kTileLocalBits)), cf[e].y));
+        }
+        const int nfaces = (int)tface.size() - fbase;
+        if (nfaces >= (1 << 15)) {
+            ok = false;
+            break;
+        }
+        // contributions in gather-list order
+        size_t bi = 0;
+        for (int c = c0; c < c1; c++) {
+            int k = 0;
+            for (int e = cptr[c]; e < cptr[c + 1]; e++, k++) {
+                int tag = cf[e].x & ((1 << kTagBits) - 1);
+                int jl = tag > TAG_RIGHT ? bnd_local[bi++] : face_local[cf[e].y];
+                contrib[((size_t)t * max_contrib + k) * T + (c - c0)] =
+                    (unsigned short)((jl << 1) | (tag == TAG_RIGHT ? 1 : 0));
+            }
+        }
+        halo.insert(halo.end(), hl.begin(), hl.end());
+        halo_ptr[t + 1] = (int)halo.size();
+        face_ptr[t + 1] = (int)tface.size();
+        max_cells = std::max(max_cells, nloc);
+        max_faces = std::max(max_faces, nfaces);
+    }
+    const size_t smem = (size_t)(8 * max_cells + 5 * max_faces) * sizeof(double);
+    S->tiles_ok = ok && smem <= 200 * 1024;
+    if (!S->tiles_ok) return;
+    cudaStream_t s = S->stream;
+    S->tile_halo_ptr.upload(halo_ptr, s);
+    S->tile_halo.upload(halo, s);
+    S->tile_face_ptr.upload(face_ptr, s);
+    S->tile_face.upload(tface, s);
+    S->tile_contrib.upload(contrib, s);
+    S->max_contrib = max_contrib;
+    S->smem_cells = max_cells;
+    S->smem_faces = max_faces;
+    S->tile_smem = smem;
+    S->tile_faces_total = (int64_t)tface.size();
+}
+
+// Morton order of approximate cell centres (mean of the cell's face centres): consecutive cells
+// form spatially compact groups, which keeps the halo of a face tile small.
+static std::vector<int> spatial_order(const e3d_mesh_desc *d) {
+    const int N = d->n_cells;
+    std::vector<double> cx(3 * (size_t)N);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int c = 0; c < N; c++) {
+        double s[3] = {0, 0, 0};
+        int n = d->cell2face_ptr[c + 1] - d->cell2face_ptr[c];
+        for (int k = d->cell2face_ptr[c]; k < d->cell2face_ptr[c + 1]; k++)
+            for (int q = 0; q < 3; q++) s[q] += d->face_center[3 * (size_t)d->cell2face[k] + q];
+        for (int q = 0; q < 3; q++) {
+            cx[3 * (size_t)c + q] = s[q] / std::max(n, 1);
+            lo[q] = std::min(lo[q], cx[3 * (size_t)c + q]);
+            hi[q] = std::max(hi[q], cx[3 * (size_t)c + q]);
+        }
+    }
+    double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+    std::vector<std::pair<uint64_t, int>> key(N);
+    for (int c = 0; c < N; c++) {
+        uint64_t qv[3];
+        for (int q = 0; q < 3; q++) {
+            double u = (cx[3 * (size_t)c + q] - lo[q]) / ext;
+            qv[q] = (uint64_t)std::min(std::max(u, 0.0) * 2097151.0, 2097151.0);
+        }
+        uint64_t m = 0;
+        for (int b = 0; b < 21; b++)
+            for (int q = 0; q < 3; q++) m |= ((qv[q] >> b) & 1ull) << (3 * b + q);
+        key[c] = {m, c};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<int> order(N);
+    for (int c = 0; c < N; c++) order[c] = key[c].second;
+    return order;
+}
+
 static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solver *S) {
     check_desc(d);
     if (!p) throw Error(E3D_ERR_INVALID_ARG, "flow parameters are NULL");
     if (p->precision != E3D_PREC_FP64_EXACT && p->precision != E3D_PREC_FP64)
         throw Error(E3D_ERR_INVALID_ARG, "precision mode not available in this build");
     if (p->scheme != E3D_SCHEME_ROE) throw Error(E3D_ERR_INVALID_ARG, "flux scheme not available in this build");
-    if (p->ordering != E3D_ORDER_NATIVE && p->ordering != E3D_ORDER_RCM)
+    if (p->ordering != E3D_ORDER_NATIVE && p->ordering != E3D_ORDER_RCM && p->ordering != E3D_ORDER_SPATIAL)
         throw Error(E3D_ERR_INVALID_ARG, "unknown cell ordering");
     if (!(p->gamma > 1.0) || !(p->cfl > 0.0) || !(p->mach >= 0.0) || !(p->cref != 0.0) || !(p->sref != 0.0))
         throw Error(E3D_ERR_INVALID_ARG, "flow parameters out of range (gamma > 1, cfl > 0, mach >= 0, cref, sref != 0)");
@@ -489,6 +727,8 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
             adj[cur[R]++] = L;
         }
         new2old = rcm_order(N, aptr, adj);
+    } else if (p->ordering == E3D_ORDER_SPATIAL) {
+        new2old = spatial_order(d);
     } else {
         std::iota(new2old.begin(), new2old.end(), 0);
     }
@@ -519,10 +759,11 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
             }
         }
     }
-    // ---- device order: cells by new index; faces and ghosts by first use in that order
+    // ---- device order: cells by new index; interior faces and ghosts by first use in that order;
+    // the geometry of boundary face with ghost slot g sits at slot Fint + g
     std::vector<int> cptr(N + 1, 0);
     std::vector<int2> cf(M);
-    std::vector<int> face_slot(F, -1), ghost_slot(G, -1);
+    std::vector<int> face_slot(F, -1);
     std::vector<double4> fgeo(F), cgeo(N);
     std::vector<int> ghost_ref(G);
     int nf = 0, ng = 0;
@@ -531,19 +772,19 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
         cptr[c + 1] = cptr[c] + (optr[o + 1] - optr[o]);
         for (int k = optr[o], j = cptr[c]; k < optr[o + 1]; k++, j++) {
             int f = lst_face[k];
-            if (face_slot[f] < 0) {
-                face_slot[f] = nf;
-                fgeo[nf] = make_double4(d->face_unit_normal[3 * (size_t)f], d->face_unit_normal[3 * (size_t)f + 1],
-                                        d->face_unit_normal[3 * (size_t)f + 2], d->face_area[f]);
-                nf++;
-            }
             int code = lst_code[k];
-            if (f >= Fint) {
-                int g = ng++;
-                ghost_slot[f - Fint] = g;
-                ghost_ref[g] = N + (f - Fint);
-                code = (g << kTagBits) | code;
+            if (face_slot[f] < 0) {
+                if (f < Fint) {
+                    face_slot[f] = nf++;
+                } else {
+                    int g = ng++;
+                    ghost_ref[g] = N + (f - Fint);
+                    face_slot[f] = Fint + g;
+                }
+                fgeo[face_slot[f]] = make_double4(d->face_unit_normal[3 * (size_t)f], d->face_unit_normal[3 * (size_t)f + 1],
+                                                  d->face_unit_normal[3 * (size_t)f + 2], d->face_area[f]);
             }
+            if (f >= Fint) code = ((face_slot[f] - Fint) << kTagBits) | code;
             cf[j] = make_int2(code, face_slot[f]);
         }
         // spectral-radius face sums in the reference's element-to-face order (TimeIntegration.cpp:209-215)
@@ -556,7 +797,10 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
         }
         cgeo[c] = make_double4(sx, sy, sz, d->cell_volume[o]);
     }
-    if (nf != F || ng != G) throw Error(E3D_ERR_INVALID_ARG, "faces not reached from any cell");
+    if (nf != Fint || ng != G) throw Error(E3D_ERR_INVALID_ARG, "faces not reached from any cell");
+
+    // ---- face tiles (tile_kernel): kTileCells consecutive cells, their halo, faces, contributions
+    build_tiles(S, cptr, cf, Fint);
 
     // ---- freestream, FlowField::Initialize (src/solver/FlowField.cpp:68-101)
     const double PI = 3.141592653589793238;
@@ -665,6 +909,7 @@ e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *p
     e3d_status st = guarded([&] {
         create_solver(mesh, params, S.get());
         set_freestream(S.get());
+        S->autotune();
     });
     if (st == E3D_OK) *out = reinterpret_cast<e3d_solver *>(S.release());
     return st;
@@ -676,6 +921,21 @@ void e3d_solver_destroy(e3d_solver *solver) {
     cudaSetDevice(S->device);
     if (S->stream) cudaStreamSynchronize(S->stream);
     delete S;
+}
+
+e3d_status e3d_solver_info_get(const e3d_solver *solver, e3d_solver_info *info) {
+    return guarded([&] {
+        if (!solver || !info) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        const Solver *S = reinterpret_cast<const Solver *>(solver);
+        std::memset(info, 0, sizeof *info);
+        info->n_cells = S->N;
+        info->n_ghosts = S->G;
+        info->n_faces = S->F;
+        info->stage_variant = S->variant;
+        info->n_variants = kStageVariants;
+        for (int v = 0; v < kStageVariants && v < 4; v++) info->variant_ms[v] = S->variant_ms[v];
+        info->device_bytes = S->device_bytes();
+    });
 }
 
 int64_t e3d_solver_state_size(const e3d_solver *solver) {
@@ -746,7 +1006,7 @@ e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double m
         if (!solver || !force || !moment) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
         Solver *S = as_solver(solver);
         E3D_CUDA(cudaSetDevice(S->device));
-        coeff_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->coeff_args(S->cur, 0, S->scratch.p));
+        coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(S->cur, 0, S->scratch.p));
         E3D_CUDA(cudaGetLastError());
         double h[6];
         E3D_CUDA(cudaMemcpyAsync(h, S->scratch.p, sizeof h, cudaMemcpyDeviceToHost, S->stream));
@@ -795,6 +1055,18 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
                                      cudaMemcpyDeviceToDevice, S->stream));
             S->cur = 0;
         }
+        if (rp->stage_kernel > 0) {
+            const int v = rp->stage_kernel - 1;
+            if (v >= kStageVariants || (v == 2 && !S->tiles_ok))
+                throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh");
+            if (v == 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem);
+            else if (v == 2) prepare_tile_fast(S->tile_smem);
+            if (v != S->variant && S->graph) {
+                cudaGraphExecDestroy(S->graph);
+                S->graph = nullptr;
+            }
+            S->variant = v;
+        }
         int64_t launches = 0;
         double stage_ms = 0.0;
         int64_t stage_launches = 0;
@@ -831,7 +1103,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
                 }
                 finalize_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->partials.p, S->n_blocks, (double)S->N,
                                                                      S->hist.p, S->ctl);
-                coeff_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
+                coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
                 E3D_CUDA(cudaGetLastError());
                 launches += 7;
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));

@@ -23,6 +23,9 @@ namespace e3d {
 enum : int { TAG_LEFT = 0, TAG_RIGHT = 1, TAG_WALL = 2, TAG_SYM = 3, TAG_FAR = 4, TAG_FROZEN = 5 };
 constexpr int kTagBits = 3;
 constexpr int kStageThreads = 256;
+constexpr int kTileCells = kStageThreads;   // cells owned by one face tile (one per thread)
+constexpr int kTileLocalBits = 10;          // local (owned + halo) cell index in a tile face entry
+constexpr unsigned short kNoContrib = 0xFFFF;
 
 struct Freestream {
     double rho, u, v, w, p, E, H, M;
@@ -65,6 +68,17 @@ struct StageArgs {
     double *__restrict__ r_out;      // [5N] reference order (residual_only)
     double *__restrict__ dt_out;     // [N]  reference order (residual_only)
     const int *__restrict__ new2old;
+    // face-tile kernel: tile t owns cells [t*kTileCells, ...); its halo cells, faces and the
+    // per-cell contribution lists (see tile_kernel)
+    const int *__restrict__ tile_halo_ptr;
+    const int *__restrict__ tile_halo;
+    const int *__restrict__ tile_face_ptr;
+    const int2 *__restrict__ tile_face;
+    const unsigned short *__restrict__ tile_contrib;
+    int max_contrib;                 // contribution slots per cell (max faces of a cell)
+    int smem_cells;                  // max owned + halo cells of a tile
+    int smem_faces;                  // max faces of a tile
+    int fint_dev;                    // geometry slots >= this are boundary faces, slot - fint_dev = ghost
 };
 
 struct Prim {
@@ -265,8 +279,7 @@ __device__ __forceinline__ void ghost_flux(const Prim &s, double nx, double ny, 
     F[4] = s.rho * s.H * V;
 }
 
-// ------------------------------------------------------------------------------ the stage
-template <bool EXACT>
+// ------------------------------------------------------------------------------ shared pieces
 __device__ __forceinline__ void block_sum_store(double v, double *dst) {
     __shared__ double warp_sums[kStageThreads / 32];
 #pragma unroll
@@ -282,8 +295,120 @@ __device__ __forceinline__ void block_sum_store(double v, double *dst) {
     }
 }
 
+// Boundary face of interior cell c (state me): updates its ghost cell (EulerSolver::updateBC,
+// src/solver/EulerSolver.cpp:201-251) and either writes the face flux to F (wall: pressure term,
+// :331-339; farfield / unclassified: physical flux of the ghost, :349-357) and returns false, or
+// leaves the mirrored ghost in gs and returns true (symmetry: Roe against the ghost, :343-346).
+__device__ __forceinline__ bool boundary_face(const StageArgs &a, int tag, double *gp, int c, const Prim &me,
+                                              const double4 &fg, double F[5], Prim &gs) {
+    const double g = a.gamma;
+    if (tag == TAG_WALL) {
+        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+        F[0] = 0;
+        F[1] = fg.x * gs.p;
+        F[2] = fg.y * gs.p;
+        F[3] = fg.z * gs.p;
+        F[4] = 0;
+        return false;
+    }
+    if (tag == TAG_SYM) {
+        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+        return true;
+    }
+    if (tag == TAG_FAR) {
+        double q2 = me.u * me.u + me.v * me.v + me.w * me.w;
+        // interior Mach as FlowField stores it (c/|u|, FlowField.cpp:157) unless the loaded state's
+        // still holds; E is exact at stage 1 (ecell), recomputed from H at later stages
+        double dM = (a.first_stage && a.ctl->minit_valid) ? a.minit[c] : sqrt(g * (me.p / me.rho)) / sqrt(q2);
+        double dE = a.first_stage ? a.ecell[c] : me.H - me.p / me.rho;
+        ghost_farfield(gp, g, a.fs, me, dM, dE, fg.x, fg.y, fg.z, gs);
+    } else {  // unclassified boundary: the ghost keeps its (freestream) state
+        double2 g0 = reinterpret_cast<const double2 *>(gp)[0];
+        double2 g1 = reinterpret_cast<const double2 *>(gp)[1];
+        double2 g2 = reinterpret_cast<const double2 *>(gp)[2];
+        gs = Prim{g0.x, g0.y, g1.x, g1.y, g2.x, gp[6]};
+    }
+    ghost_flux(gs, fg.x, fg.y, fg.z, F);
+    return false;
+}
+
+// Time step, Runge-Kutta update and primitive recovery of cell c from its residual R; returns
+// this cell's R_rho^2 on the last stage (for the RMS), else 0.
 template <bool EXACT>
-__global__ void __launch_bounds__(kStageThreads) stage_kernel(StageArgs a) {
+__device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const Prim &me, double r_me,
+                                              const double R[5]) {
+    const double g = a.gamma;
+    // local time step, TimeStepMethod2 (src/solver/TimeIntegration.cpp:8-40)
+    const double4 cg = a.cgeo[c];
+    double lam, dt;
+    if (EXACT) {
+        double snd = sqrt(g * me.p / me.rho);
+        double lx = 0.5 * (fabs(me.u) + snd) * cg.x;
+        double ly = 0.5 * (fabs(me.v) + snd) * cg.y;
+        double lz = 0.5 * (fabs(me.w) + snd) * cg.z;
+        lam = lx + ly + lz;
+        dt = a.cfl * cg.w / lam;
+    } else {
+        double snd = g * me.p * r_me;
+        lam = 0.5 * ((fabs(me.u) + snd) * cg.x + (fabs(me.v) + snd) * cg.y + (fabs(me.w) + snd) * cg.z);
+        dt = a.cfl * cg.w / lam;
+    }
+    if (a.residual_only) {
+        const int o = a.new2old[c];
+#pragma unroll
+        for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
+        a.dt_out[o] = dt;
+        return 0.0;
+    }
+    // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
+    const size_t N = (size_t)a.n_cells;
+    double W[5];
+    if (EXACT) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - a.alpha * dt * R[k] / cg.w;
+    } else {
+        double coef = a.alpha * a.cfl / lam;  // alpha dt / V
+#pragma unroll
+        for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - coef * R[k];
+    }
+    Prim s;
+    double E;
+    s.rho = W[0];
+    if (EXACT) {
+        s.u = W[1] / s.rho;
+        s.v = W[2] / s.rho;
+        s.w = W[3] / s.rho;
+        E = W[4] / s.rho;
+        double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+        s.p = (g - 1) * s.rho * (E - q2 / 2.0);
+        s.H = E + (s.p / s.rho);
+    } else {
+        double ir = 1.0 / s.rho;
+        s.u = W[1] * ir;
+        s.v = W[2] * ir;
+        s.w = W[3] * ir;
+        E = W[4] * ir;
+        s.p = (g - 1.0) * (W[4] - 0.5 * (W[1] * s.u + W[2] * s.v + W[3] * s.w));
+        s.H = (W[4] + s.p) * ir;
+    }
+    store_prim(a.qout, c, s);
+    if (!a.last_stage) return 0.0;
+    // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
+    a.w0[0 * N + c] = s.rho;
+    a.w0[1 * N + c] = s.u * s.rho;
+    a.w0[2 * N + c] = s.v * s.rho;
+    a.w0[3 * N + c] = s.w * s.rho;
+    a.w0[4 * N + c] = E * s.rho;
+    a.ecell[c] = E;
+    return R[0] * R[0];
+}
+
+// ------------------------------------------------------------------------------ gather kernel
+// One thread per cell; the cell walks its own faces and evaluates each flux itself (an interior
+// face is evaluated by both of its cells).  MINB: resident blocks per SM the register allocation
+// must allow (an occupancy variant the autotuner chooses per mesh).
+template <bool EXACT, int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a) {
     if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
     const int c = blockIdx.x * kStageThreads + threadIdx.x;
     const double g = a.gamma;
@@ -304,125 +429,135 @@ __global__ void __launch_bounds__(kStageThreads) stage_kernel(StageArgs a) {
             const int idx = ent.x >> kTagBits;
             const double4 fg = a.fgeo[ent.y];
             double F[5];
+            // Operands of the Roe flux in (left, right) order.  Interior faces select them per lane
+            // instead of branching, so a warp whose cells sit on either side of their faces runs one
+            // flux evaluation, not two.  The right cell subtracts F*S as F*(-S) (same IEEE result).
+            Prim fl, fr;
+            double sS = fg.w;
+            bool roe = true;
+            double s_l = s_me, s_r = s_me, r_l = r_me;
             if (tag <= TAG_RIGHT) {
                 const Prim nb = load_prim(a.qin, idx);
-                if (EXACT) {
-                    if (tag == TAG_LEFT) roe_exact(me, nb, fg.x, fg.y, fg.z, g, F);
-                    else roe_exact(nb, me, fg.x, fg.y, fg.z, g, F);
-                } else {
+                const bool left = tag == TAG_LEFT;
+                fl = left ? me : nb;
+                fr = left ? nb : me;
+                sS = left ? fg.w : -fg.w;
+                if (!EXACT) {
                     double s_nb = sqrt(nb.rho);
-                    if (tag == TAG_LEFT) roe_fast(me, nb, s_me, s_nb, r_me, fg.x, fg.y, fg.z, g, F);
-                    else roe_fast(nb, me, s_nb, s_me, rsqrt(g * nb.p * nb.rho), fg.x, fg.y, fg.z, g, F);
+                    s_l = left ? s_me : s_nb;
+                    s_r = left ? s_nb : s_me;
+                    r_l = left ? r_me : rsqrt(g * nb.p * nb.rho);
                 }
-                if (tag == TAG_LEFT) {
-#pragma unroll
-                    for (int k = 0; k < 5; k++) R[k] += F[k] * fg.w;
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 5; k++) R[k] -= F[k] * fg.w;
-                }
-                continue;
-            }
-            double *gp = a.ghost + 8 * (size_t)idx;
-            Prim gs;
-            if (tag == TAG_WALL) {  // ghost mirrored; flux is the pressure term only (EulerSolver.cpp:331-339)
-                ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
-                F[0] = 0;
-                F[1] = fg.x * gs.p;
-                F[2] = fg.y * gs.p;
-                F[3] = fg.z * gs.p;
-                F[4] = 0;
-            } else if (tag == TAG_SYM) {  // Roe against the mirrored ghost (:343-346)
-                ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
-                if (EXACT) roe_exact(me, gs, fg.x, fg.y, fg.z, g, F);
-                else roe_fast(me, gs, s_me, s_me, r_me, fg.x, fg.y, fg.z, g, F);  // mirrored rho == rho_me
             } else {
-                if (tag == TAG_FAR) {
-                    double q2 = me.u * me.u + me.v * me.v + me.w * me.w;
-                    // Mach as FlowField stores it (c/|u|, FlowField.cpp:157) unless the loaded state's
-                    // still holds; E is exact at stage 1 (ecell), recomputed from H at later stages
-                    double dM = (a.first_stage && a.ctl->minit_valid) ? a.minit[c] : sqrt(g * (me.p / me.rho)) / sqrt(q2);
-                    double dE = a.first_stage ? a.ecell[c] : me.H - me.p / me.rho;
-                    ghost_farfield(gp, g, a.fs, me, dM, dE, fg.x, fg.y, fg.z, gs);
-                } else {  // unclassified boundary: the ghost keeps its (freestream) state
-                    double2 g0 = reinterpret_cast<const double2 *>(gp)[0];
-                    double2 g1 = reinterpret_cast<const double2 *>(gp)[1];
-                    double2 g2 = reinterpret_cast<const double2 *>(gp)[2];
-                    gs = Prim{g0.x, g0.y, g1.x, g1.y, g2.x, gp[6]};
-                }
-                ghost_flux(gs, fg.x, fg.y, fg.z, F);  // (:349-357)
+                Prim gs;
+                roe = boundary_face(a, tag, a.ghost + 8 * (size_t)idx, c, me, fg, F, gs);
+                fl = me;
+                fr = gs;  // symmetry ghost: rho and p are the cell's, so s_r = s_me
+            }
+            if (roe) {
+                if (EXACT) roe_exact(fl, fr, fg.x, fg.y, fg.z, g, F);
+                else roe_fast(fl, fr, s_l, s_r, r_l, fg.x, fg.y, fg.z, g, F);
             }
 #pragma unroll
-            for (int k = 0; k < 5; k++) R[k] += F[k] * fg.w;
+            for (int k = 0; k < 5; k++) R[k] += F[k] * sS;
         }
+        r2 = finish_cell<EXACT>(a, c, me, r_me, R);
+    }
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+}
 
-        // local time step, TimeStepMethod2 (src/solver/TimeIntegration.cpp:8-40)
-        const double4 cg = a.cgeo[c];
-        double lam, dt;
-        if (EXACT) {
-            double snd = sqrt(g * me.p / me.rho);
-            double lx = 0.5 * (fabs(me.u) + snd) * cg.x;
-            double ly = 0.5 * (fabs(me.v) + snd) * cg.y;
-            double lz = 0.5 * (fabs(me.w) + snd) * cg.z;
-            lam = lx + ly + lz;
-            dt = a.cfl * cg.w / lam;
-        } else {
-            double snd = g * me.p * r_me;
-            lam = 0.5 * ((fabs(me.u) + snd) * cg.x + (fabs(me.v) + snd) * cg.y + (fabs(me.w) + snd) * cg.z);
-            dt = a.cfl * cg.w / lam;
-        }
+// ------------------------------------------------------------------------------ face-tile kernel
+// One block per tile of kTileCells consecutive cells (a spatially compact group in the Morton
+// cell order).  Phase 1 stages the states of the tile's cells and of their outside neighbours
+// (halo) in shared memory with all loads in flight at once; phase 2 evaluates every face touching
+// the tile once (faces shared with another tile are evaluated by both) and keeps F*S in shared
+// memory; phase 3 gives each cell the sum of its faces' F*S in ascending reference face id, the
+// order of the reference's face loop, so results are deterministic and, in exact mode, identical
+// to the reference.
+//   tile_face[j].x = l | r << 10 | tag << 20 (local cell indices; r unused for boundary faces)
+//   tile_face[j].y = geometry slot (boundary faces: fint_dev + ghost slot)
+//   tile_contrib[(t * max_contrib + k) * kTileCells + i] = local face << 1 | (cell is the right one)
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ double smem[];
+    const int LC = a.smem_cells, FC = a.smem_faces;
+    double *qs = smem;             // 8 x LC: rho u v w p H sqrt(rho) rsqrt(gamma p rho)
+    double *fs = smem + 8 * LC;    // 5 x FC: F*S per tile face
+    const int tile = blockIdx.x, c0 = tile * kTileCells;
+    const int nloc = min(kTileCells, a.n_cells - c0);
+    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
+    const int f0 = a.tile_face_ptr[tile], nf = a.tile_face_ptr[tile + 1] - f0;
+    const double g = a.gamma;
 
-        if (a.residual_only) {
-            const int o = a.new2old[c];
-#pragma unroll
-            for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
-            a.dt_out[o] = dt;
-            return;
-        }
-
-        // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
-        const size_t N = (size_t)a.n_cells;
-        double W[5];
-        if (EXACT) {
-#pragma unroll
-            for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - a.alpha * dt * R[k] / cg.w;
-        } else {
-            double coef = a.alpha * a.cfl / lam;  // alpha dt / V
-#pragma unroll
-            for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - coef * R[k];
-        }
-        Prim s;
-        double E;
-        s.rho = W[0];
-        if (EXACT) {
-            s.u = W[1] / s.rho;
-            s.v = W[2] / s.rho;
-            s.w = W[3] / s.rho;
-            E = W[4] / s.rho;
-            double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
-            s.p = (g - 1) * s.rho * (E - q2 / 2.0);
-            s.H = E + (s.p / s.rho);
-        } else {
-            double ir = 1.0 / s.rho;
-            s.u = W[1] * ir;
-            s.v = W[2] * ir;
-            s.w = W[3] * ir;
-            E = W[4] * ir;
-            s.p = (g - 1.0) * (W[4] - 0.5 * (W[1] * s.u + W[2] * s.v + W[3] * s.w));
-            s.H = (W[4] + s.p) * ir;
-        }
-        store_prim(a.qout, c, s);
-        if (a.last_stage) {  // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
-            a.w0[0 * N + c] = s.rho;
-            a.w0[1 * N + c] = s.u * s.rho;
-            a.w0[2 * N + c] = s.v * s.rho;
-            a.w0[3 * N + c] = s.w * s.rho;
-            a.w0[4 * N + c] = E * s.rho;
-            a.ecell[c] = E;
-            r2 = R[0] * R[0];
+    // phase 1: owned cells (coalesced) and halo cells (gathered)
+    for (int i = threadIdx.x; i < nloc + nh; i += kStageThreads) {
+        const int cg = i < nloc ? c0 + i : a.tile_halo[h0 + i - nloc];
+        const Prim q = load_prim(a.qin, cg);
+        qs[0 * LC + i] = q.rho;
+        qs[1 * LC + i] = q.u;
+        qs[2 * LC + i] = q.v;
+        qs[3 * LC + i] = q.w;
+        qs[4 * LC + i] = q.p;
+        qs[5 * LC + i] = q.H;
+        if (!EXACT) {
+            qs[6 * LC + i] = sqrt(q.rho);
+            qs[7 * LC + i] = rsqrt(g * q.p * q.rho);
         }
     }
-    if (a.last_stage && !a.residual_only) block_sum_store<EXACT>(r2, a.partials + blockIdx.x);
+    __syncthreads();
+    auto local_prim = [&](int i) {
+        return Prim{qs[i], qs[LC + i], qs[2 * LC + i], qs[3 * LC + i], qs[4 * LC + i], qs[5 * LC + i]};
+    };
+
+    // phase 2: one flux per tile face
+    for (int j = threadIdx.x; j < nf; j += kStageThreads) {
+        const int2 ent = a.tile_face[f0 + j];
+        const int l = ent.x & ((1 << kTileLocalBits) - 1);
+        const int r = (ent.x >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
+        const int tag = ent.x >> (2 * kTileLocalBits);
+        const double4 fg = a.fgeo[ent.y];
+        const Prim L = local_prim(l);
+        double F[5];
+        if (tag == TAG_LEFT) {
+            const Prim R = local_prim(r);
+            if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
+            else roe_fast(L, R, qs[6 * LC + l], qs[6 * LC + r], qs[7 * LC + l], fg.x, fg.y, fg.z, g, F);
+        } else {
+            Prim gs;
+            double *gp = a.ghost + 8 * (size_t)(ent.y - a.fint_dev);
+            if (boundary_face(a, tag, gp, c0 + l, L, fg, F, gs)) {
+                if (EXACT) roe_exact(L, gs, fg.x, fg.y, fg.z, g, F);
+                else roe_fast(L, gs, qs[6 * LC + l], qs[6 * LC + l], qs[7 * LC + l], fg.x, fg.y, fg.z, g, F);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 5; k++) fs[k * FC + j] = F[k] * fg.w;
+    }
+    __syncthreads();
+
+    // phase 3: each owned cell sums its contributions and is updated
+    double r2 = 0.0;
+    const int i = threadIdx.x;
+    if (i < nloc) {
+        const Prim me = local_prim(i);
+        double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        const unsigned short *ct = a.tile_contrib + (size_t)tile * a.max_contrib * kTileCells + i;
+        for (int k = 0; k < a.max_contrib; k++) {
+            const unsigned short e = ct[k * kTileCells];
+            if (e == kNoContrib) break;
+            const int j = e >> 1;
+            if (e & 1) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) R[q] -= fs[q * FC + j];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; q++) R[q] += fs[q * FC + j];
+            }
+        }
+        r2 = finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : qs[7 * LC + i], R);
+    }
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
 }  // namespace e3d

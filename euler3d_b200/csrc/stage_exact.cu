@@ -1,12 +1,26 @@
-// FP64_EXACT instantiation of the stage kernel.  Built with -fmad=false so that every double
+// FP64_EXACT instantiations of the stage kernels.  Built with -fmad=false so that every double
 // operation rounds exactly as the reference's source order does.
 #include "stage.cuh"
 
 namespace e3d {
 
-void launch_stage_exact(const StageArgs &a, cudaStream_t s) {
+// Dynamic shared memory the tile kernel may use (set once per process before launches).
+void prepare_tile_exact(size_t smem_bytes) {
+    cudaFuncSetAttribute(tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+}
+
+// variant 0: gather kernel, 1 block(s)/SM register budget; 1: gather kernel, 2 blocks/SM;
+// 2: face-tile kernel
+void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
-    stage_kernel<true><<<blocks, kStageThreads, 0, s>>>(a);
+    if (variant == 2) {
+        const size_t smem = (size_t)(8 * a.smem_cells + 5 * a.smem_faces) * sizeof(double);
+        tile_kernel<true><<<blocks, kStageThreads, smem, s>>>(a);
+    } else if (variant == 1) {
+        stage_kernel<true, 2><<<blocks, kStageThreads, 0, s>>>(a);
+    } else {
+        stage_kernel<true, 1><<<blocks, kStageThreads, 0, s>>>(a);
+    }
 }
 
 }  // namespace e3d

@@ -1,11 +1,25 @@
-// FP64 instantiation of the stage kernel: restructured arithmetic, FMA contraction allowed.
+// FP64 instantiations of the stage kernels: restructured arithmetic, FMA contraction allowed.
 #include "stage.cuh"
 
 namespace e3d {
 
-void launch_stage_fast(const StageArgs &a, cudaStream_t s) {
+// Dynamic shared memory the tile kernel may use (set once per process before launches).
+void prepare_tile_fast(size_t smem_bytes) {
+    cudaFuncSetAttribute(tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+}
+
+// variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;
+// 2: face-tile kernel
+void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
-    stage_kernel<false><<<blocks, kStageThreads, 0, s>>>(a);
+    if (variant == 2) {
+        const size_t smem = (size_t)(8 * a.smem_cells + 5 * a.smem_faces) * sizeof(double);
+        tile_kernel<false><<<blocks, kStageThreads, smem, s>>>(a);
+    } else if (variant == 1) {
+        stage_kernel<false, 3><<<blocks, kStageThreads, 0, s>>>(a);
+    } else {
+        stage_kernel<false, 2><<<blocks, kStageThreads, 0, s>>>(a);
+    }
 }
 
 }  // namespace e3d

@@ -198,6 +198,13 @@ class EulerSolver:
         except Exception:
             pass
 
+    def info(self) -> Dict[str, object]:
+        i = _lib.SolverInfo()
+        check(_lib.load().e3d_solver_info_get(self._h, C.byref(i)))
+        return {"n_cells": i.n_cells, "n_ghosts": i.n_ghosts, "n_faces": i.n_faces,
+                "stage_variant": i.stage_variant, "variant_ms": list(i.variant_ms)[: i.n_variants],
+                "device_bytes": i.device_bytes}
+
     # ---- state
     def set_state(self, state: Dict[str, np.ndarray]) -> None:
         arrs = [np.ascontiguousarray(state[k], np.float64) for k in STATE_KEYS]
@@ -218,8 +225,9 @@ class EulerSolver:
 
     # ---- hot path
     def run(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
-            check_every: int = 0, profile_stages: bool = False) -> Dict[str, object]:
-        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages))
+            check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0) -> Dict[str, object]:
+        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages),
+                            stage_kernel)
         st = _lib.RunStats()
         status = _lib.load().e3d_solver_run(self._h, C.byref(rp), C.byref(st))
         stats = {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,

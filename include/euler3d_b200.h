@@ -51,8 +51,10 @@ enum { E3D_SCHEME_ROE = 0, E3D_SCHEME_AUSM = 1 };
  *                state, Runge-Kutta accumulation and all reductions in double. */
 enum { E3D_PREC_FP64_EXACT = 0, E3D_PREC_FP64 = 1, E3D_PREC_FP32_FLUX = 2 };
 
-/* Cell ordering used on the device (results are always returned in reference order). */
-enum { E3D_ORDER_NATIVE = 0, E3D_ORDER_RCM = 1 };
+/* Cell ordering used on the device (results are always returned in reference order):
+ * reference order, reverse Cuthill-McKee of the cell graph, or Morton order of the cell centres
+ * (spatially compact groups of cells, which the face-tile kernel needs). */
+enum { E3D_ORDER_NATIVE = 0, E3D_ORDER_RCM = 1, E3D_ORDER_SPATIAL = 2 };
 
 /* Why e3d_solver_run stopped (the exits of EulerSolver::Run, src/solver/EulerSolver.cpp:100-152). */
 enum { E3D_STOP_MAX_ITER = 0, E3D_STOP_RESIDUAL = 1, E3D_STOP_COEFFICIENTS = 2 };
@@ -146,6 +148,18 @@ typedef struct e3d_solver e3d_solver;
 e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *params, e3d_solver **out);
 void e3d_solver_destroy(e3d_solver *solver);
 
+/* What the handle holds on the device and what its autotuner chose.  At creation the solver times
+ * each compiled variant of the stage kernel (register budget / occupancy) on this mesh, with
+ * writes redirected to scratch, and keeps the fastest. */
+typedef struct e3d_solver_info {
+	int32_t n_cells, n_ghosts, n_faces;
+	int32_t stage_variant;            /* variant in use */
+	int32_t n_variants;
+	float variant_ms[4];              /* measured duration of one stage launch per variant */
+	int64_t device_bytes;             /* device memory held by the handle */
+} e3d_solver_info;
+e3d_status e3d_solver_info_get(const e3d_solver *solver, e3d_solver_info *info);
+
 /* Number of entries of each state array: n_cells + (n_faces - n_faces_int). */
 int64_t e3d_solver_state_size(const e3d_solver *solver);
 
@@ -164,6 +178,8 @@ typedef struct e3d_run_params {
 	                                     stop flag (0: 32); iterations past a stop are no-ops */
 	int32_t profile_stages;           /* 1: launch directly and time every stage kernel with CUDA
 	                                     events (stats.stage_ms); 0: CUDA graphs */
+	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
+	                                     register budgets; 3: face tiles (kept for later runs) */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {

@@ -42,14 +42,21 @@ def assert_state_equal(gpu, ora, n_cells, ghost_E_rtol=0.0):
             assert diff.size == 0, f"{k}: {diff.size} entries differ, first {diff[:5]}"
 
 
+KERNELS = [_lib.KERNEL_GATHER, _lib.KERNEL_GATHER_B, _lib.KERNEL_TILE]
+ORDERINGS = [_lib.ORDER_NATIVE, _lib.ORDER_RCM, _lib.ORDER_SPATIAL]
+
+
 @pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
-@pytest.mark.parametrize("ordering", [_lib.ORDER_NATIVE, _lib.ORDER_RCM])
-def test_residual_bitwise(name, ordering):
-    """updateBC + computeResidual + updateDeltaTime on a perturbed state, every BC branch."""
+@pytest.mark.parametrize("ordering", ORDERINGS)
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_residual_bitwise(name, ordering, kernel):
+    """updateBC + computeResidual + updateDeltaTime on a perturbed state, every BC branch, every
+    stage-kernel variant and cell ordering."""
     flow = CASES[name].flow(precision=_lib.PREC_FP64_EXACT, ordering=ordering)
     arrays, m, fl = oracle_setup(name, flow)
     st = perturbed_state(arrays, flow, seed=11)
     s = EulerSolver(arrays, flow)
+    s.run(0, stage_kernel=kernel)  # select the variant
     s.set_state(st)
     R, dt = s.residual()
     gpu = s.get_state()
@@ -63,14 +70,15 @@ def test_residual_bitwise(name, ordering):
 
 
 @pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
-def test_rk_iteration_bitwise(name):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_rk_iteration_bitwise(name, kernel):
     """One full RK5 iteration (EulerSolver::Run body) from a perturbed state."""
-    flow = CASES[name].flow(precision=_lib.PREC_FP64_EXACT)
+    flow = CASES[name].flow(precision=_lib.PREC_FP64_EXACT, ordering=_lib.ORDER_SPATIAL)
     arrays, m, fl = oracle_setup(name, flow)
     st = perturbed_state(arrays, flow, seed=12)
     s = EulerSolver(arrays, flow)
     s.set_state(st)
-    stats = s.run(1)
+    stats = s.run(1, stage_kernel=kernel)
     gpu = s.get_state()
     o = po.State(m, st)
     ost, ohist = po.run(m, fl, o, 1)
@@ -81,19 +89,20 @@ def test_rk_iteration_bitwise(name):
 
 
 @pytest.mark.parametrize("name", ["c1", "tets", "ogrid"])
-def test_100_iterations(name):
+@pytest.mark.parametrize("kernel", [_lib.KERNEL_GATHER, _lib.KERNEL_TILE])
+def test_100_iterations(name, kernel):
     """100 iterations from the freestream: exact mode bit for bit, fast mode within 1e-10."""
-    fl_exact = CASES[name].flow(precision=_lib.PREC_FP64_EXACT, ordering=_lib.ORDER_RCM)
+    fl_exact = CASES[name].flow(precision=_lib.PREC_FP64_EXACT, ordering=_lib.ORDER_SPATIAL)
     arrays, m, fl = oracle_setup(name, fl_exact)
     o = po.freestream(m, fl)
     ost, ohist = po.run(m, fl, o, 100)
     s = EulerSolver(arrays, fl_exact)
-    stats = s.run(100)
+    stats = s.run(100, stage_kernel=kernel)
     assert stats["iterations"] == 100
     assert_state_equal(s.get_state(), o.a, m.n_cells, ghost_E_rtol=1e-13)
     assert rel_err(s.rms_history(), ohist) <= RMS_RTOL
-    fast = EulerSolver(arrays, CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_RCM))
-    fast.run(100)
+    fast = EulerSolver(arrays, CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL))
+    fast.run(100, stage_kernel=kernel)
     g = fast.get_state()
     speed = np.sqrt(o.a["u"] ** 2 + o.a["v"] ** 2 + o.a["w"] ** 2)
     for k in ("rho", "u", "v", "w", "p", "E", "H"):
@@ -186,15 +195,41 @@ def test_nonfinite_reported():
     assert s.run(2)["iterations"] == 2
 
 
-def test_determinism():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_determinism(kernel):
     name = "ogrid"
-    flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_RCM)
+    flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
     arrays = prepared(name)
     out = []
     for _ in range(2):
         s = EulerSolver(arrays, flow)
-        s.run(20)
+        s.run(20, stage_kernel=kernel)
         out.append((s.get_state(), s.rms_history()))
     for k in STATE_KEYS:
         assert np.array_equal(out[0][0][k], out[1][0][k])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_fast_kernels_agree():
+    """The three FP64 stage kernels give the same state to round-off (different FMA grouping
+    and, for the tiles, per-face instead of per-cell sqrt reuse)."""
+    name = "tets"
+    flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
+    arrays = prepared(name)
+    states = []
+    for kernel in KERNELS:
+        s = EulerSolver(arrays, flow)
+        s.run(30, stage_kernel=kernel)
+        states.append(s.get_state())
+    for k in ("rho", "p", "H"):
+        for other in states[1:]:
+            assert np.max(np.abs(other[k] - states[0][k]) / np.abs(states[0][k])) < 1e-12
+
+
+def test_autotune_info():
+    name = "tets"
+    s = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL))
+    info = s.info()
+    assert len(info["variant_ms"]) == 3 and 0 <= info["stage_variant"] < 3
+    assert all(t > 0 for t in info["variant_ms"])
+    assert info["variant_ms"][info["stage_variant"]] == min(info["variant_ms"])
