@@ -181,10 +181,10 @@ __global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
 // Reference-ordered FlowField arrays (staging, 8 x T) -> device layout.
 __global__ void load_state_kernel(const double *__restrict__ st, int64_t T, int n_cells, int n_ghosts,
                                   const int *__restrict__ new2old, const int *__restrict__ ghost_ref,
-                                  double2 *__restrict__ q, double *__restrict__ w0, double *__restrict__ ecell,
-                                  double *__restrict__ minit, double *__restrict__ ghost) {
+                                  double2 *__restrict__ q, double *__restrict__ w0, int w0_stride,
+                                  double *__restrict__ ecell, double *__restrict__ minit, double *__restrict__ ghost) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t N = (size_t)n_cells;
+    const size_t N = (size_t)w0_stride;
     if (i < n_cells) {
         int o = new2old[i];
         double rho = st[o], u = st[T + o], v = st[2 * T + o], w = st[3 * T + o];
@@ -300,8 +300,10 @@ struct Solver {
     std::vector<int> new2old, ghost_ref;  // host copies of the maps
 
     DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell, tile_halo_ptr, tile_halo, tile_face_ptr;
-    DevBuf<int2> tile_face;
+    DevBuf<FaceRec> tile_rec;
+    DevBuf<long long> tile_rec_off;
     DevBuf<unsigned short> tile_contrib;
+    int w0_stride = 0;
     bool tiles_ok = false;
     int max_contrib = 0, smem_cells = 0, smem_faces = 0;
     size_t tile_smem = 0;
@@ -328,7 +330,8 @@ struct Solver {
             if (e) cudaEventDestroy(e);
         DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell, &tile_halo_ptr, &tile_halo, &tile_face_ptr};
         for (auto *b : ib) b->release();
-        tile_face.release();
+        tile_rec.release();
+        tile_rec_off.release();
         tile_contrib.release();
         cf.release();
         fgeo.release();
@@ -347,7 +350,8 @@ struct Solver {
 
     int64_t device_bytes() const {
         return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
-                         tile_face_ptr.n) * 4 + (int64_t)(cf.n + tile_face.n) * 8 + (int64_t)tile_contrib.n * 2 +
+                         tile_face_ptr.n) * 4 + (int64_t)cf.n * 8 + (int64_t)tile_rec.n * 40 + (int64_t)tile_rec_off.n * 8 +
+               (int64_t)tile_contrib.n * 2 +
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
                          hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
@@ -379,12 +383,14 @@ struct Solver {
         a.tile_halo_ptr = tile_halo_ptr.p;
         a.tile_halo = tile_halo.p;
         a.tile_face_ptr = tile_face_ptr.p;
-        a.tile_face = tile_face.p;
+        a.tile_rec = reinterpret_cast<const char *>(tile_rec.p);
+        a.tile_rec_off = tile_rec_off.p;
         a.tile_contrib = tile_contrib.p;
         a.max_contrib = max_contrib;
         a.smem_cells = smem_cells;
         a.smem_faces = smem_faces;
-        a.fint_dev = Fint;
+        a.w0_stride = w0_stride;
+        a.fault = &ctl->fault;
         return a;
     }
 
@@ -517,11 +523,13 @@ static void check_desc(const e3d_mesh_desc *d) {
 // an owned cell (once, interior ones before boundary ones) and its owned cells' boundary faces; each
 // owned cell lists its faces in the order of its gather list (ascending reference face id).  Tiles
 // whose local cells or faces exceed the entry encoding leave the variant disabled.
-static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vector<int2> &cf, int Fint) {
+static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vector<int2> &cf,
+                        const std::vector<double4> &fgeo, int Fint) {
     const int N = S->N, T = kTileCells;
     const int n_tiles = (N + T - 1) / T;
     std::vector<int> halo_ptr(n_tiles + 1, 0), halo, face_ptr(n_tiles + 1, 0);
-    std::vector<int2> tface;
+    std::vector<long long> rec_off(n_tiles + 1, 0);
+    std::vector<FaceRec> tface;
     int max_contrib = 0;
     for (int c = 0; c < N; c++) max_contrib = std::max(max_contrib, cptr[c + 1] - cptr[c]);
     std::vector<unsigned short> contrib((size_t)n_tiles * max_contrib * T, kNoContrib);
@@ -549,7 +557,7 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
             ok = false;
             break;
         }
-        const int fbase = (int)tface.size();
+        const int fbase = (int)tface.size();  // tile blocks are padded, so fbase is rec_off[t] / 40
         bnd.clear();
         // interior faces first (one entry per face), boundary faces after
         for (int c = c0; c < c1; c++)
@@ -566,7 +574,9 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
                 int nb = cf[e].x >> kTagBits;
                 int l = tag == TAG_LEFT ? local(c) : local(nb);
                 int r = tag == TAG_LEFT ? local(nb) : local(c);
-                tface.push_back(make_int2(l | (r << kTileLocalBits) | (TAG_LEFT << (2 * kTileLocalBits)), slot));
+                const double4 gq = fgeo[slot];
+                tface.push_back(FaceRec{l | (r << kTileLocalBits) | (TAG_LEFT << (2 * kTileLocalBits)), -1, gq.x, gq.y,
+                                        gq.z, gq.w});
             }
         std::vector<int> bnd_local(bnd.size());
         for (size_t b = 0; b < bnd.size(); b++) {
@@ -574,7 +584,8 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
             int tag = cf[e].x & ((1 << kTagBits) - 1);
             int c = (int)(std::upper_bound(cptr.begin(), cptr.end(), e) - cptr.begin()) - 1;
             bnd_local[b] = (int)tface.size() - fbase;
-            tface.push_back(make_int2(local(c) | (tag << (2 * kTileLocalBits)), cf[e].y));
+            const double4 gq = fgeo[cf[e].y];
+            tface.push_back(FaceRec{local(c) | (tag << (2 * kTileLocalBits)), cf[e].y - Fint, gq.x, gq.y, gq.z, gq.w});
         }
         const int nfaces = (int)tface.size() - fbase;
         if (nfaces >= (1 << 15)) {
@@ -594,18 +605,21 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
         }
         halo.insert(halo.end(), hl.begin(), hl.end());
         halo_ptr[t + 1] = (int)halo.size();
-        face_ptr[t + 1] = (int)tface.size();
+        face_ptr[t + 1] = face_ptr[t] + nfaces;
+        while ((tface.size() * sizeof(FaceRec)) % 16) tface.push_back(FaceRec{0, -1, 0, 0, 0, 0});  // 16-byte blocks
+        rec_off[t + 1] = (long long)(tface.size() * sizeof(FaceRec));
         max_cells = std::max(max_cells, nloc);
         max_faces = std::max(max_faces, nfaces);
     }
-    const size_t smem = (size_t)(8 * max_cells + 5 * max_faces) * sizeof(double);
+    const size_t smem = tile_smem_bytes(max_cells, max_faces, max_contrib);
     S->tiles_ok = ok && smem <= 200 * 1024;
     if (!S->tiles_ok) return;
     cudaStream_t s = S->stream;
     S->tile_halo_ptr.upload(halo_ptr, s);
     S->tile_halo.upload(halo, s);
     S->tile_face_ptr.upload(face_ptr, s);
-    S->tile_face.upload(tface, s);
+    S->tile_rec.upload(tface, s);
+    S->tile_rec_off.upload(rec_off, s);
     S->tile_contrib.upload(contrib, s);
     S->max_contrib = max_contrib;
     S->smem_cells = max_cells;
@@ -800,7 +814,7 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     if (nf != Fint || ng != G) throw Error(E3D_ERR_INVALID_ARG, "faces not reached from any cell");
 
     // ---- face tiles (tile_kernel): kTileCells consecutive cells, their halo, faces, contributions
-    build_tiles(S, cptr, cf, Fint);
+    build_tiles(S, cptr, cf, fgeo, Fint);
 
     // ---- freestream, FlowField::Initialize (src/solver/FlowField.cpp:68-101)
     const double PI = 3.141592653589793238;
@@ -842,7 +856,8 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     S->wall_center.upload(wct, s);
     S->q[0].alloc(3 * (size_t)N);
     S->q[1].alloc(3 * (size_t)N);
-    S->w0.alloc(5 * (size_t)N);
+    S->w0_stride = (N + 31) / 32 * 32;
+    S->w0.alloc(5 * (size_t)S->w0_stride);
     S->ecell.alloc(N);
     S->minit.alloc(N);
     S->ghost.alloc(8 * (size_t)std::max(G, 1));
@@ -868,8 +883,8 @@ static void upload_state(Solver *S, const double *const *arr) {
     }
     int threads = 256, blocks = (int)((T + threads - 1) / threads);
     load_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
-                                                         S->ghost_ref_d.p, S->q[0].p, S->w0.p, S->ecell.p,
-                                                         S->minit.p, S->ghost.p);
+                                                         S->ghost_ref_d.p, S->q[0].p, S->w0.p, S->w0_stride,
+                                                         S->ecell.p, S->minit.p, S->ghost.p);
     E3D_CUDA(cudaGetLastError());
     S->cur = 0;
     Control init{};
@@ -1140,6 +1155,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         st.stage_ms = stage_ms;
         st.stage_launches = stage_launches;
         if (stats) *stats = st;
+        if (c.fault) throw Error(E3D_ERR_TIMEOUT, "a bounded device wait gave up (asynchronous copy did not complete)");
         if (c.nonfinite)
             throw Error(E3D_ERR_NONFINITE, "density residual became NaN/Inf at iteration " + std::to_string(c.it));
     });

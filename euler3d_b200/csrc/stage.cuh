@@ -11,7 +11,8 @@
 //   fgeo[F]           double4 (unit normal x,y,z ; area)
 //   cgeo[N]           double4 (sum|Sx|, sum|Sy|, sum|Sz| over the cell's faces ; volume)
 //   q[2][3N]          double2 x3 per cell: (rho,u) (v,w) (p,H), ping-pong between stages
-//   w0[5N]            conservative state at the start of the RK step (SoA)
+//   w0[5 x stride]    conservative state at the start of the RK step (SoA, stride = N rounded up
+//                     to 32 so that every tile's segment is 16-byte aligned for bulk copies)
 //   ecell[N]          energy E of the last completed RK step (or of the loaded state)
 //   ghost[8G]         ghost cells, 8 doubles each: rho u v w p E H M
 #pragma once
@@ -41,7 +42,8 @@ struct Control {
     int sample_now;    // this iteration samples the force coefficients
     int minit_valid;   // interior Mach of the loaded state still holds (no stage has run since)
     int nonfinite;     // the RMS became NaN/Inf
-    int max_iter, sampling, hist_cap, pad;
+    int max_iter, sampling, hist_cap;
+    int fault;         // a bounded wait in a kernel gave up
     double min_res, min_aero, last_rms, cl, cd, cm;
     double force[3], moment[3];
 };
@@ -68,18 +70,29 @@ struct StageArgs {
     double *__restrict__ r_out;      // [5N] reference order (residual_only)
     double *__restrict__ dt_out;     // [N]  reference order (residual_only)
     const int *__restrict__ new2old;
-    // face-tile kernel: tile t owns cells [t*kTileCells, ...); its halo cells, faces and the
-    // per-cell contribution lists (see tile_kernel)
+    int w0_stride;                   // row stride of w0
+    // face-tile kernel: tile t owns cells [t*kTileCells, ...); its halo cells, face records and
+    // the per-cell contribution lists (see tile_kernel)
     const int *__restrict__ tile_halo_ptr;
     const int *__restrict__ tile_halo;
-    const int *__restrict__ tile_face_ptr;
-    const int2 *__restrict__ tile_face;
+    const int *__restrict__ tile_face_ptr;   // face count of tile t = ptr[t+1] - ptr[t]
+    const char *__restrict__ tile_rec;       // FaceRec blocks, one 16-byte aligned block per tile
+    const long long *__restrict__ tile_rec_off;  // byte offset of tile t's block
     const unsigned short *__restrict__ tile_contrib;
     int max_contrib;                 // contribution slots per cell (max faces of a cell)
     int smem_cells;                  // max owned + halo cells of a tile
     int smem_faces;                  // max faces of a tile
-    int fint_dev;                    // geometry slots >= this are boundary faces, slot - fint_dev = ghost
+    int *fault;                      // set when a bounded wait gives up (reported as a timeout)
 };
+
+// One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
+// faces), ghost slot for boundary faces, unit normal and area.
+struct FaceRec {
+    int code;
+    int ghost;
+    double nx, ny, nz, S;
+};
+static_assert(sizeof(FaceRec) == 40, "FaceRec layout");
 
 struct Prim {
     double rho, u, v, w, p, H;
@@ -332,14 +345,13 @@ __device__ __forceinline__ bool boundary_face(const StageArgs &a, int tag, doubl
     return false;
 }
 
-// Time step, Runge-Kutta update and primitive recovery of cell c from its residual R; returns
-// this cell's R_rho^2 on the last stage (for the RMS), else 0.
+// Time step, Runge-Kutta update and primitive recovery of cell c from its residual R, the cell's
+// W0 and geometry; returns this cell's R_rho^2 on the last stage (for the RMS), else 0.
 template <bool EXACT>
 __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const Prim &me, double r_me,
-                                              const double R[5]) {
+                                              const double R[5], const double W0[5], const double4 cg) {
     const double g = a.gamma;
     // local time step, TimeStepMethod2 (src/solver/TimeIntegration.cpp:8-40)
-    const double4 cg = a.cgeo[c];
     double lam, dt;
     if (EXACT) {
         double snd = sqrt(g * me.p / me.rho);
@@ -361,15 +373,14 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         return 0.0;
     }
     // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
-    const size_t N = (size_t)a.n_cells;
     double W[5];
     if (EXACT) {
 #pragma unroll
-        for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - a.alpha * dt * R[k] / cg.w;
+        for (int k = 0; k < 5; k++) W[k] = W0[k] - a.alpha * dt * R[k] / cg.w;
     } else {
         double coef = a.alpha * a.cfl / lam;  // alpha dt / V
 #pragma unroll
-        for (int k = 0; k < 5; k++) W[k] = a.w0[k * N + c] - coef * R[k];
+        for (int k = 0; k < 5; k++) W[k] = W0[k] - coef * R[k];
     }
     Prim s;
     double E;
@@ -394,11 +405,12 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
     store_prim(a.qout, c, s);
     if (!a.last_stage) return 0.0;
     // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
-    a.w0[0 * N + c] = s.rho;
-    a.w0[1 * N + c] = s.u * s.rho;
-    a.w0[2 * N + c] = s.v * s.rho;
-    a.w0[3 * N + c] = s.w * s.rho;
-    a.w0[4 * N + c] = E * s.rho;
+    const size_t st = (size_t)a.w0_stride;
+    a.w0[0 * st + c] = s.rho;
+    a.w0[1 * st + c] = s.u * s.rho;
+    a.w0[2 * st + c] = s.v * s.rho;
+    a.w0[3 * st + c] = s.w * s.rho;
+    a.w0[4 * st + c] = E * s.rho;
     a.ecell[c] = E;
     return R[0] * R[0];
 }
@@ -461,74 +473,153 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
 #pragma unroll
             for (int k = 0; k < 5; k++) R[k] += F[k] * sS;
         }
-        r2 = finish_cell<EXACT>(a, c, me, r_me, R);
+        double W0[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c];
+        r2 = finish_cell<EXACT>(a, c, me, r_me, R, W0, a.cgeo[c]);
     }
     if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
+// ------------------------------------------------------------------------------ async copies
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bulk (TMA) copy global -> this CTA's shared memory, completing on bar.  dst, src 16-byte
+// aligned, bytes a multiple of 16.  No multicast.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n cp.async.wait_group 0;" ::: "memory");
+}
+
+constexpr int kWaitLimit = 1 << 22;  // polls of a barrier before the kernel gives up and reports
+
+__device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
+
 // ------------------------------------------------------------------------------ face-tile kernel
 // One block per tile of kTileCells consecutive cells (a spatially compact group in the Morton
-// cell order).  Phase 1 stages the states of the tile's cells and of their outside neighbours
-// (halo) in shared memory with all loads in flight at once; phase 2 evaluates every face touching
-// the tile once (faces shared with another tile are evaluated by both) and keeps F*S in shared
-// memory; phase 3 gives each cell the sum of its faces' F*S in ascending reference face id, the
-// order of the reference's face loop, so results are deterministic and, in exact mode, identical
-// to the reference.
-//   tile_face[j].x = l | r << 10 | tag << 20 (local cell indices; r unused for boundary faces)
-//   tile_face[j].y = geometry slot (boundary faces: fint_dev + ghost slot)
-//   tile_contrib[(t * max_contrib + k) * kTileCells + i] = local face << 1 | (cell is the right one)
+// cell order).
+//   Load: one thread issues bulk copies of every contiguous per-tile segment (owned states, face
+//   records with their geometry, W0, cell geometry, contribution lists) onto an mbarrier, while all
+//   threads gather the halo states (outside neighbours) with cp.async; one bounded wait.
+//   Phase 2: every face touching the tile is evaluated once (a face shared with another tile is
+//   evaluated by both) and F*S kept in shared memory.
+//   Phase 3: each cell sums its faces' F*S in ascending reference face id, the order of the
+//   reference's face loop, so results are deterministic and, in exact mode, the reference's.
+// Shared memory: st[LC] 48-byte states | rec[FC] | w0[5][T] | cg[T] | contrib[MC][T] | fs[5][FC]
+//               | sqrt(rho), rsqrt(gamma p rho) [2][LC] (fast path) | mbarrier
 template <bool EXACT>
 __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
     if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ double smem[];
-    const int LC = a.smem_cells, FC = a.smem_faces;
-    double *qs = smem;             // 8 x LC: rho u v w p H sqrt(rho) rsqrt(gamma p rho)
-    double *fs = smem + 8 * LC;    // 5 x FC: F*S per tile face
-    const int tile = blockIdx.x, c0 = tile * kTileCells;
-    const int nloc = min(kTileCells, a.n_cells - c0);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
+    double2 *st = reinterpret_cast<double2 *>(smem_raw);
+    FaceRec *rec = reinterpret_cast<FaceRec *>(smem_raw + (size_t)LC * 48);
+    double *w0s = reinterpret_cast<double *>(smem_raw + (size_t)LC * 48 + round16(40u * FC));
+    double4 *cgs = reinterpret_cast<double4 *>(w0s + 5 * T);
+    unsigned short *cts = reinterpret_cast<unsigned short *>(cgs + T);
+    double *fs = reinterpret_cast<double *>(cts + (size_t)MC * T);
+    double *sq = fs + 5 * FC;  // 2 x LC
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+
+    const int tile = blockIdx.x, c0 = tile * T;
+    const int nloc = min(T, a.n_cells - c0);
     const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
-    const int f0 = a.tile_face_ptr[tile], nf = a.tile_face_ptr[tile + 1] - f0;
+    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
     const double g = a.gamma;
 
-    // phase 1: owned cells (coalesced) and halo cells (gathered)
-    for (int i = threadIdx.x; i < nloc + nh; i += kStageThreads) {
-        const int cg = i < nloc ? c0 + i : a.tile_halo[h0 + i - nloc];
-        const Prim q = load_prim(a.qin, cg);
-        qs[0 * LC + i] = q.rho;
-        qs[1 * LC + i] = q.u;
-        qs[2 * LC + i] = q.v;
-        qs[3 * LC + i] = q.w;
-        qs[4 * LC + i] = q.p;
-        qs[5 * LC + i] = q.H;
-        if (!EXACT) {
-            qs[6 * LC + i] = sqrt(q.rho);
-            qs[7 * LC + i] = rsqrt(g * q.p * q.rho);
-        }
-    }
+    if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
-    auto local_prim = [&](int i) {
-        return Prim{qs[i], qs[LC + i], qs[2 * LC + i], qs[3 * LC + i], qs[4 * LC + i], qs[5 * LC + i]};
+    if (threadIdx.x == 0) {
+        const uint32_t b_state = (uint32_t)nloc * 48u;
+        const uint32_t b_rec = round16(40u * (uint32_t)nf);
+        const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // reads past the tile stay inside the padded rows
+        const uint32_t b_cg = (uint32_t)nloc * 32u;
+        const uint32_t b_ct = (uint32_t)MC * T * 2u;
+        mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
+        bulk_g2s(st, a.qin + 3 * (size_t)c0, b_state, bar);
+        bulk_g2s(rec, a.tile_rec + a.tile_rec_off[tile], b_rec, bar);
+        for (int k = 0; k < 5; k++) bulk_g2s(w0s + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
+        bulk_g2s(cgs, a.cgeo + c0, b_cg, bar);
+        bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+    }
+    for (int i = threadIdx.x; i < nh; i += kStageThreads) {
+        const int h = a.tile_halo[h0 + i];
+        const double2 *src = a.qin + 3 * (size_t)h;
+        double2 *dst = st + 3 * (nloc + i);
+        cp_async16(dst, src);
+        cp_async16(dst + 1, src + 1);
+        cp_async16(dst + 2, src + 2);
+    }
+    cp_async_wait_all();
+    bool ok = false;
+    for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, 0);
+    if (!ok) atomicExch(a.fault, 1);
+    if (__syncthreads_or(!ok)) {
+        // give the copies in flight a last bounded chance to land before the block leaves
+        for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, 0);
+        return;
+    }
+    auto prim = [&](int i) {
+        const double2 x = st[3 * i], y = st[3 * i + 1], z = st[3 * i + 2];
+        return Prim{x.x, x.y, y.x, y.y, z.x, z.y};
     };
+    if (!EXACT) {
+        for (int i = threadIdx.x; i < nloc + nh; i += kStageThreads) {
+            const Prim q = prim(i);
+            sq[i] = sqrt(q.rho);
+            sq[LC + i] = rsqrt(g * q.p * q.rho);
+        }
+        __syncthreads();
+    }
 
     // phase 2: one flux per tile face
     for (int j = threadIdx.x; j < nf; j += kStageThreads) {
-        const int2 ent = a.tile_face[f0 + j];
-        const int l = ent.x & ((1 << kTileLocalBits) - 1);
-        const int r = (ent.x >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
-        const int tag = ent.x >> (2 * kTileLocalBits);
-        const double4 fg = a.fgeo[ent.y];
-        const Prim L = local_prim(l);
+        const FaceRec fr = rec[j];
+        const int l = fr.code & ((1 << kTileLocalBits) - 1);
+        const int r = (fr.code >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
+        const int tag = fr.code >> (2 * kTileLocalBits);
+        const double4 fg = make_double4(fr.nx, fr.ny, fr.nz, fr.S);
+        const Prim L = prim(l);
         double F[5];
         if (tag == TAG_LEFT) {
-            const Prim R = local_prim(r);
+            const Prim R = prim(r);
             if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
-            else roe_fast(L, R, qs[6 * LC + l], qs[6 * LC + r], qs[7 * LC + l], fg.x, fg.y, fg.z, g, F);
+            else roe_fast(L, R, sq[l], sq[r], sq[LC + l], fg.x, fg.y, fg.z, g, F);
         } else {
             Prim gs;
-            double *gp = a.ghost + 8 * (size_t)(ent.y - a.fint_dev);
+            double *gp = a.ghost + 8 * (size_t)fr.ghost;
             if (boundary_face(a, tag, gp, c0 + l, L, fg, F, gs)) {
                 if (EXACT) roe_exact(L, gs, fg.x, fg.y, fg.z, g, F);
-                else roe_fast(L, gs, qs[6 * LC + l], qs[6 * LC + l], qs[7 * LC + l], fg.x, fg.y, fg.z, g, F);
+                else roe_fast(L, gs, sq[l], sq[l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
             }
         }
 #pragma unroll
@@ -540,11 +631,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
     double r2 = 0.0;
     const int i = threadIdx.x;
     if (i < nloc) {
-        const Prim me = local_prim(i);
+        const Prim me = prim(i);
         double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        const unsigned short *ct = a.tile_contrib + (size_t)tile * a.max_contrib * kTileCells + i;
-        for (int k = 0; k < a.max_contrib; k++) {
-            const unsigned short e = ct[k * kTileCells];
+        for (int k = 0; k < MC; k++) {
+            const unsigned short e = cts[k * T + i];
             if (e == kNoContrib) break;
             const int j = e >> 1;
             if (e & 1) {
@@ -555,9 +645,22 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
                 for (int q = 0; q < 5; q++) R[q] += fs[q * FC + j];
             }
         }
-        r2 = finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : qs[7 * LC + i], R);
+        double W0[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) W0[k] = w0s[k * T + i];
+        r2 = finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : sq[LC + i], R, W0, cgs[i]);
     }
     if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+}
+
+// Dynamic shared memory of tile_kernel for the given maxima.
+inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
+    size_t b = (size_t)smem_cells * 48 + ((40u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
+               kTileCells * 32 + (size_t)max_contrib * kTileCells * 2;
+    b = (b + 15) & ~(size_t)15;
+    b += 5 * (size_t)smem_faces * 8 + 2 * (size_t)smem_cells * 8;
+    b = (b + 15) & ~(size_t)15;
+    return b + 16;
 }
 
 }  // namespace e3d

@@ -13,7 +13,7 @@ void prepare_tile_fast(size_t smem_bytes) {
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
     if (variant == 2) {
-        const size_t smem = (size_t)(8 * a.smem_cells + 5 * a.smem_faces) * sizeof(double);
+        const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 1) {
         stage_kernel<false, 3><<<blocks, kStageThreads, 0, s>>>(a);
