@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="hexahedra per box edge (6 tets each)")
     ap.add_argument("--precision", choices=["fp64", "fp64_exact"], default="fp64")
     ap.add_argument("--ordering", choices=["spatial", "rcm", "native"], default="spatial")
-    ap.add_argument("--kernel", type=int, default=0, help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles")
+    ap.add_argument("--kernel", type=int, default=0, help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined face tiles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -256,7 +256,8 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>"][solver.info()["stage_variant"]],
+                     "kernel": ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>",
+                                "tile_pipe_kernel<false>"][solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "autotune": solver.info()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,

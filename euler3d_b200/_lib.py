@@ -15,7 +15,7 @@ E3D_OK, E3D_ERR_INVALID_ARG, E3D_ERR_OOM, E3D_ERR_NONFINITE, E3D_ERR_TIMEOUT, E3
 SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
 ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE = 0, 1, 2, 3, 4
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)

@@ -20,9 +20,9 @@ namespace e3d {
 
 void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant);
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
-void prepare_tile_exact(size_t smem_bytes);
-void prepare_tile_fast(size_t smem_bytes);
-constexpr int kStageVariants = 3;  // gather (two register budgets), face tile
+void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
+void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
+constexpr int kStageVariants = 4;  // gather (two register budgets), face tiles, pipelined face tiles
 
 constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
@@ -304,7 +304,10 @@ struct Solver {
     DevBuf<long long> tile_rec_off;
     DevBuf<unsigned short> tile_contrib;
     int w0_stride = 0;
-    bool tiles_ok = false;
+    int prefetch_distance = 0;  // tile_kernel L2 prefetch distance: resident blocks on the device
+    bool tiles_ok = false, pipe_ok = false;
+    size_t pipe_smem = 0;
+    int n_tiles = 0, n_sm = 0;
     int max_contrib = 0, smem_cells = 0, smem_faces = 0;
     size_t tile_smem = 0;
     int64_t tile_faces_total = 0;
@@ -391,6 +394,9 @@ struct Solver {
         a.smem_faces = smem_faces;
         a.w0_stride = w0_stride;
         a.fault = &ctl->fault;
+        a.prefetch_distance = prefetch_distance;
+        a.n_tiles = n_tiles;
+        a.pipe_grid = std::min(n_tiles, n_sm);
         return a;
     }
 
@@ -416,12 +422,12 @@ struct Solver {
         const int reps = N > 200000 ? 3 : 10;
         float best = 1e30f;
         if (tiles_ok) {
-            if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem);
-            else prepare_tile_fast(tile_smem);
+            if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
+            else prepare_tile_fast(tile_smem, pipe_smem);
         }
         for (int v = 0; v < kStageVariants; v++) {
             variant_ms[v] = -1.0f;
-            if (v == 2 && !tiles_ok) continue;
+            if ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok)) continue;
             launch_stage(a, v);  // warm
             E3D_CUDA(cudaEventRecord(ev0, stream));
             for (int r = 0; r < reps; r++) launch_stage(a, v);
@@ -612,7 +618,13 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
         max_faces = std::max(max_faces, nfaces);
     }
     const size_t smem = tile_smem_bytes(max_cells, max_faces, max_contrib);
+    S->n_tiles = n_tiles;
     S->tiles_ok = ok && smem <= 200 * 1024;
+    int max_halo = 0;
+    for (int t = 0; t < n_tiles; t++) max_halo = std::max(max_halo, halo_ptr[t + 1] - halo_ptr[t]);
+    S->pipe_smem = tile_smem_bytes(max_cells, max_faces, max_contrib, 2);
+    S->pipe_ok = S->tiles_ok && S->pipe_smem <= 227 * 1024 && max_halo <= kPipeThreads;
+    if (!S->pipe_ok) S->pipe_smem = 0;
     if (!S->tiles_ok) return;
     cudaStream_t s = S->stream;
     S->tile_halo_ptr.upload(halo_ptr, s);
@@ -687,6 +699,8 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     E3D_CUDA(cudaSetDevice(p->device));
     S->device = p->device;
     S->prm = *p;
+    S->prefetch_distance = 2 * prop.multiProcessorCount;  // two resident tile blocks per SM
+    S->n_sm = prop.multiProcessorCount;
     if (p->stream) {
         S->stream = (cudaStream_t)p->stream;
     } else {
@@ -1072,10 +1086,10 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         }
         if (rp->stage_kernel > 0) {
             const int v = rp->stage_kernel - 1;
-            if (v >= kStageVariants || (v == 2 && !S->tiles_ok))
+            if (v >= kStageVariants || (v == 2 && !S->tiles_ok) || (v == 3 && !S->pipe_ok))
                 throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh");
-            if (v == 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem);
-            else if (v == 2) prepare_tile_fast(S->tile_smem);
+            if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);
+            else if (v >= 2) prepare_tile_fast(S->tile_smem, S->pipe_smem);
             if (v != S->variant && S->graph) {
                 cudaGraphExecDestroy(S->graph);
                 S->graph = nullptr;

@@ -83,6 +83,9 @@ struct StageArgs {
     int smem_cells;                  // max owned + halo cells of a tile
     int smem_faces;                  // max faces of a tile
     int *fault;                      // set when a bounded wait gives up (reported as a timeout)
+    int prefetch_distance;           // tile_kernel: tiles ahead whose data each block prefetches into L2
+    int n_tiles;                     // tiles of the mesh
+    int pipe_grid;                   // tile_pipe_kernel: persistent blocks (one per SM)
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -107,6 +110,41 @@ __device__ __forceinline__ void store_prim(double2 *__restrict__ q, int c, const
     q[3 * c] = make_double2(s.rho, s.u);
     q[3 * c + 1] = make_double2(s.v, s.w);
     q[3 * c + 2] = make_double2(s.p, s.H);
+}
+
+// ------------------------------------------------------------------------------ fast reciprocals
+// FP64 path only (never FP64_EXACT): reciprocal and reciprocal square root from the single-
+// precision hardware approximations (PTX rcp.approx.ftz.f32 / rsqrt.approx.ftz.f32, relative error
+// below 2^-22) refined by two Newton-Raphson steps, each of which squares the relative error
+// (Markstein, "Computation of elementary functions on the IBM RISC System/6000 processor",
+// IBM J. Res. Dev. 34, 1990).  The result is within about one unit in the last place.  Arguments
+// outside [1e-30, 1e30] (where the single-precision seed would flush or overflow), zero, NaN
+// and Inf take the IEEE double operation instead.
+__device__ __forceinline__ bool seed_range(double x) {
+    const double ax = fabs(x);
+    return ax > 1e-30 && ax < 1e30;
+}
+
+__device__ __forceinline__ double rcp_nr(double x) {
+    if (!seed_range(x)) return 1.0 / x;
+    float xf = (float)x, yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+    double y = (double)yf;
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    if (!(x > 1e-30 && x < 1e30)) return rsqrt(x);
+    float xf = (float)x, yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+    double y = (double)yf;
+    double hx = 0.5 * x;
+    y = y * fma(-hx * y, y, 1.5);
+    y = y * fma(-hx * y, y, 1.5);
+    return y;
 }
 
 // ------------------------------------------------------------------------------ Roe flux
@@ -171,7 +209,7 @@ __device__ __forceinline__ void roe_exact(const Prim &L, const Prim &R, double n
 // from the caller (each is computed once per cell where possible).
 __device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl, double sr, double rcl,
                                          double nx, double ny, double nz, double g, double F[5]) {
-    double inv = 1.0 / (sl + sr);
+    double inv = rcp_nr(sl + sr);
     double wl = sl * inv, wr = sr * inv;
     double ut = L.u * wl + R.u * wr;
     double vt = L.v * wl + R.v * wr;
@@ -180,7 +218,7 @@ __device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl
     double rt = sl * sr;
     double q2t = ut * ut + vt * vt + wt * wt;
     double c2 = (g - 1.0) * (ht - 0.5 * q2t);
-    double rc = rsqrt(c2);
+    double rc = rsqrt_nr(c2);
     double ct = c2 * rc, ic2 = rc * rc;
     double Vt = ut * nx + vt * ny + wt * nz;
     double Vl = L.u * nx + L.v * ny + L.w * nz;
@@ -293,15 +331,16 @@ __device__ __forceinline__ void ghost_flux(const Prim &s, double nx, double ny, 
 }
 
 // ------------------------------------------------------------------------------ shared pieces
+template <int NT = kStageThreads>
 __device__ __forceinline__ void block_sum_store(double v, double *dst) {
-    __shared__ double warp_sums[kStageThreads / 32];
+    __shared__ double warp_sums[NT / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) warp_sums[wid] = v;
     __syncthreads();
     if (wid == 0) {
-        v = lane < kStageThreads / 32 ? warp_sums[lane] : 0.0;
+        v = lane < NT / 32 ? warp_sums[lane] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) *dst = v;
@@ -363,7 +402,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
     } else {
         double snd = g * me.p * r_me;
         lam = 0.5 * ((fabs(me.u) + snd) * cg.x + (fabs(me.v) + snd) * cg.y + (fabs(me.w) + snd) * cg.z);
-        dt = a.cfl * cg.w / lam;
+        dt = a.residual_only ? a.cfl * cg.w / lam : 0.0;  // the update below needs only alpha*cfl/lam
     }
     if (a.residual_only) {
         const int o = a.new2old[c];
@@ -378,7 +417,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
 #pragma unroll
         for (int k = 0; k < 5; k++) W[k] = W0[k] - a.alpha * dt * R[k] / cg.w;
     } else {
-        double coef = a.alpha * a.cfl / lam;  // alpha dt / V
+        double coef = a.alpha * a.cfl * rcp_nr(lam);  // alpha dt / V
 #pragma unroll
         for (int k = 0; k < 5; k++) W[k] = W0[k] - coef * R[k];
     }
@@ -394,7 +433,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         s.p = (g - 1) * s.rho * (E - q2 / 2.0);
         s.H = E + (s.p / s.rho);
     } else {
-        double ir = 1.0 / s.rho;
+        double ir = rcp_nr(s.rho);
         s.u = W[1] * ir;
         s.v = W[2] * ir;
         s.w = W[3] * ir;
@@ -430,8 +469,8 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
         // sqrt(rho) and rsqrt(gamma p rho) of this cell, shared by all its faces (fast path)
         double s_me = 0.0, r_me = 0.0;
         if (!EXACT) {
-            s_me = sqrt(me.rho);
-            r_me = rsqrt(g * me.p * me.rho);
+            s_me = me.rho * rsqrt_nr(me.rho);
+            r_me = rsqrt_nr(g * me.p * me.rho);
         }
         double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         const int e0 = a.cptr[c], e1 = a.cptr[c + 1];
@@ -455,10 +494,10 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
                 fr = left ? nb : me;
                 sS = left ? fg.w : -fg.w;
                 if (!EXACT) {
-                    double s_nb = sqrt(nb.rho);
+                    double s_nb = nb.rho * rsqrt_nr(nb.rho);
                     s_l = left ? s_me : s_nb;
                     s_r = left ? s_nb : s_me;
-                    r_l = left ? r_me : rsqrt(g * nb.p * nb.rho);
+                    r_l = left ? r_me : rsqrt_nr(g * nb.p * nb.rho);
                 }
             } else {
                 Prim gs;
@@ -512,6 +551,13 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
+// Bulk prefetch of a global range into L2 (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -524,94 +570,97 @@ constexpr int kWaitLimit = 1 << 22;  // polls of a barrier before the kernel giv
 
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
-// ------------------------------------------------------------------------------ face-tile kernel
-// One block per tile of kTileCells consecutive cells (a spatially compact group in the Morton
-// cell order).
-//   Load: one thread issues bulk copies of every contiguous per-tile segment (owned states, face
-//   records with their geometry, W0, cell geometry, contribution lists) onto an mbarrier, while all
-//   threads gather the halo states (outside neighbours) with cp.async; one bounded wait.
-//   Phase 2: every face touching the tile is evaluated once (a face shared with another tile is
-//   evaluated by both) and F*S kept in shared memory.
-//   Phase 3: each cell sums its faces' F*S in ascending reference face id, the order of the
-//   reference's face loop, so results are deterministic and, in exact mode, the reference's.
-// Shared memory: st[LC] 48-byte states | rec[FC] | w0[5][T] | cg[T] | contrib[MC][T] | fs[5][FC]
-//               | sqrt(rho), rsqrt(gamma p rho) [2][LC] (fast path) | mbarrier
-template <bool EXACT>
-__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
-    double2 *st = reinterpret_cast<double2 *>(smem_raw);
-    FaceRec *rec = reinterpret_cast<FaceRec *>(smem_raw + (size_t)LC * 48);
-    double *w0s = reinterpret_cast<double *>(smem_raw + (size_t)LC * 48 + round16(40u * FC));
-    double4 *cgs = reinterpret_cast<double4 *>(w0s + 5 * T);
-    unsigned short *cts = reinterpret_cast<unsigned short *>(cgs + T);
-    double *fs = reinterpret_cast<double *>(cts + (size_t)MC * T);
-    double *sq = fs + 5 * FC;  // 2 x LC
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+// ------------------------------------------------------------------------------ face tiles
+// A tile is kTileCells consecutive cells (a spatially compact group in the Morton cell order).
+// Its data, staged in shared memory:
+//   st[LC]   48-byte states: owned cells (one bulk copy) then halo cells (outside neighbours,
+//            gathered with cp.async)
+//   rec[FC]  FaceRec of every face touching the tile (one bulk copy)
+//   w0[5][T], cg[T], ct[MC][T]   W0, cell geometry and contribution lists (bulk copies)
+// Evaluation: every face touching the tile is evaluated once (a face shared with another tile is
+// evaluated by both) and F*S kept in fs[5][FC]; each cell then sums its faces' F*S in ascending
+// reference face id, the order of the reference's face loop, so results are deterministic and, in
+// exact mode, the reference's bit for bit.
+struct TileBuf {
+    double2 *st;
+    FaceRec *rec;
+    double *w0;
+    double4 *cg;
+    unsigned short *ct;
+};
 
-    const int tile = blockIdx.x, c0 = tile * T;
-    const int nloc = min(T, a.n_cells - c0);
-    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
+__device__ __forceinline__ size_t tile_buf_bytes(int LC, int FC, int MC) {
+    return (size_t)LC * 48 + ((40u * (size_t)FC + 15) & ~(size_t)15) + 5 * kTileCells * 8 + kTileCells * 32 +
+           (size_t)MC * kTileCells * 2;
+}
+
+__device__ __forceinline__ TileBuf tile_buf_at(unsigned char *base, int LC, int FC, int MC) {
+    TileBuf b;
+    b.st = reinterpret_cast<double2 *>(base);
+    b.rec = reinterpret_cast<FaceRec *>(base + (size_t)LC * 48);
+    b.w0 = reinterpret_cast<double *>(base + (size_t)LC * 48 + round16(40u * FC));
+    b.cg = reinterpret_cast<double4 *>(b.w0 + 5 * kTileCells);
+    b.ct = reinterpret_cast<unsigned short *>(b.cg + kTileCells);
+    return b;
+}
+
+// Thread `lead` issues the tile's bulk copies onto bar (expecting their byte count).
+__device__ __forceinline__ void tile_issue_bulk(const StageArgs &a, int tile, const TileBuf &b, uint64_t *bar) {
+    const int T = kTileCells, MC = a.max_contrib;
+    const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
     const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+    const uint32_t b_state = (uint32_t)nloc * 48u;
+    const uint32_t b_rec = round16(40u * (uint32_t)nf);
+    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // reads past the tile stay inside the padded rows
+    const uint32_t b_cg = (uint32_t)nloc * 32u;
+    const uint32_t b_ct = (uint32_t)MC * T * 2u;
+    mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
+    bulk_g2s(b.st, a.qin + 3 * (size_t)c0, b_state, bar);
+    bulk_g2s(b.rec, a.tile_rec + a.tile_rec_off[tile], b_rec, bar);
+    for (int k = 0; k < 5; k++) bulk_g2s(b.w0 + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
+    bulk_g2s(b.cg, a.cgeo + c0, b_cg, bar);
+    bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+}
+
+// Halo state i of the tile (global cell h) into st[nloc + i] with three 16-byte cp.async.
+__device__ __forceinline__ void tile_gather_halo(const StageArgs &a, const TileBuf &b, int nloc, int i, int h) {
+    const double2 *src = a.qin + 3 * (size_t)h;
+    double2 *dst = b.st + 3 * (nloc + i);
+    cp_async16(dst, src);
+    cp_async16(dst + 1, src + 1);
+    cp_async16(dst + 2, src + 2);
+}
+
+__device__ __forceinline__ Prim tile_prim(const double2 *st, int i) {
+    const double2 x = st[3 * i], y = st[3 * i + 1], z = st[3 * i + 2];
+    return Prim{x.x, x.y, y.x, y.y, z.x, z.y};
+}
+
+// sqrt(rho) and rsqrt(gamma p rho) of the tile's cells (fast path only).
+template <int NT>
+__device__ __forceinline__ void tile_roots(const StageArgs &a, const TileBuf &b, double *sq, int LC, int ncells) {
+    for (int i = threadIdx.x; i < ncells; i += NT) {
+        const Prim q = tile_prim(b.st, i);
+        sq[i] = q.rho * rsqrt_nr(q.rho);
+        sq[LC + i] = rsqrt_nr(a.gamma * q.p * q.rho);
+    }
+}
+
+// One flux per tile face, F*S into fs.
+template <bool EXACT, int NT>
+__device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, const double *sq, double *fs,
+                                            int LC, int FC, int nf, int c0) {
     const double g = a.gamma;
-
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t b_state = (uint32_t)nloc * 48u;
-        const uint32_t b_rec = round16(40u * (uint32_t)nf);
-        const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // reads past the tile stay inside the padded rows
-        const uint32_t b_cg = (uint32_t)nloc * 32u;
-        const uint32_t b_ct = (uint32_t)MC * T * 2u;
-        mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
-        bulk_g2s(st, a.qin + 3 * (size_t)c0, b_state, bar);
-        bulk_g2s(rec, a.tile_rec + a.tile_rec_off[tile], b_rec, bar);
-        for (int k = 0; k < 5; k++) bulk_g2s(w0s + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
-        bulk_g2s(cgs, a.cgeo + c0, b_cg, bar);
-        bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
-    }
-    for (int i = threadIdx.x; i < nh; i += kStageThreads) {
-        const int h = a.tile_halo[h0 + i];
-        const double2 *src = a.qin + 3 * (size_t)h;
-        double2 *dst = st + 3 * (nloc + i);
-        cp_async16(dst, src);
-        cp_async16(dst + 1, src + 1);
-        cp_async16(dst + 2, src + 2);
-    }
-    cp_async_wait_all();
-    bool ok = false;
-    for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, 0);
-    if (!ok) atomicExch(a.fault, 1);
-    if (__syncthreads_or(!ok)) {
-        // give the copies in flight a last bounded chance to land before the block leaves
-        for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, 0);
-        return;
-    }
-    auto prim = [&](int i) {
-        const double2 x = st[3 * i], y = st[3 * i + 1], z = st[3 * i + 2];
-        return Prim{x.x, x.y, y.x, y.y, z.x, z.y};
-    };
-    if (!EXACT) {
-        for (int i = threadIdx.x; i < nloc + nh; i += kStageThreads) {
-            const Prim q = prim(i);
-            sq[i] = sqrt(q.rho);
-            sq[LC + i] = rsqrt(g * q.p * q.rho);
-        }
-        __syncthreads();
-    }
-
-    // phase 2: one flux per tile face
-    for (int j = threadIdx.x; j < nf; j += kStageThreads) {
-        const FaceRec fr = rec[j];
+    for (int j = threadIdx.x; j < nf; j += NT) {
+        const FaceRec fr = b.rec[j];
         const int l = fr.code & ((1 << kTileLocalBits) - 1);
         const int r = (fr.code >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
         const int tag = fr.code >> (2 * kTileLocalBits);
         const double4 fg = make_double4(fr.nx, fr.ny, fr.nz, fr.S);
-        const Prim L = prim(l);
+        const Prim L = tile_prim(b.st, l);
         double F[5];
         if (tag == TAG_LEFT) {
-            const Prim R = prim(r);
+            const Prim R = tile_prim(b.st, r);
             if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
             else roe_fast(L, R, sq[l], sq[r], sq[LC + l], fg.x, fg.y, fg.z, g, F);
         } else {
@@ -625,40 +674,185 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
 #pragma unroll
         for (int k = 0; k < 5; k++) fs[k * FC + j] = F[k] * fg.w;
     }
-    __syncthreads();
+}
 
-    // phase 3: each owned cell sums its contributions and is updated
-    double r2 = 0.0;
-    const int i = threadIdx.x;
-    if (i < nloc) {
-        const Prim me = prim(i);
-        double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int k = 0; k < MC; k++) {
-            const unsigned short e = cts[k * T + i];
-            if (e == kNoContrib) break;
-            const int j = e >> 1;
-            if (e & 1) {
+// Cell i of the tile: sum of its contributions, then time step and update; returns R_rho^2 on
+// the last stage.  The contribution entries and W0 / geometry loads are issued before the sums.
+template <bool EXACT>
+__device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf &b, const double *sq,
+                                              const double *fs, int LC, int FC, int c0, int i) {
+    const int T = kTileCells;
+    double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    unsigned short e[6];
 #pragma unroll
-                for (int q = 0; q < 5; q++) R[q] -= fs[q * FC + j];
-            } else {
+    for (int k = 0; k < 6; k++) e[k] = k < a.max_contrib ? b.ct[k * T + i] : kNoContrib;
+    double W0[5];
 #pragma unroll
-                for (int q = 0; q < 5; q++) R[q] += fs[q * FC + j];
-            }
+    for (int k = 0; k < 5; k++) W0[k] = b.w0[k * T + i];
+    const double4 cg = b.cg[i];
+    const Prim me = tile_prim(b.st, i);
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        if (e[k] == kNoContrib) break;
+        const int j = e[k] >> 1;
+        if (e[k] & 1) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) R[q] -= fs[q * FC + j];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; q++) R[q] += fs[q * FC + j];
         }
-        double W0[5];
-#pragma unroll
-        for (int k = 0; k < 5; k++) W0[k] = w0s[k * T + i];
-        r2 = finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : sq[LC + i], R, W0, cgs[i]);
     }
+    return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : sq[LC + i], R, W0, cg);
+}
+
+// Bounded wait on an mbarrier phase by every thread; on timeout the fault word is set.
+// Returns true for the whole block only if every thread saw the phase complete.
+__device__ __forceinline__ bool tile_wait(const StageArgs &a, uint64_t *bar, uint32_t parity) {
+    bool ok = false;
+    for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, parity);
+    if (!ok) atomicExch(a.fault, 1);
+    return !__syncthreads_or(!ok);
+}
+
+// ---- one block per tile, all loads issued at the start (variant 2)
+// Shared memory: TileBuf | fs[5][FC] | sq[2][LC] | mbarrier
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
+    const TileBuf b = tile_buf_at(smem_raw, LC, FC, MC);
+    size_t off = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
+    double *fs = reinterpret_cast<double *>(smem_raw + off);
+    double *sq = fs + 5 * FC;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+
+    const int tile = blockIdx.x, c0 = tile * T;
+    const int nloc = min(T, a.n_cells - c0);
+    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
+    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) tile_issue_bulk(a, tile, b, bar);
+    for (int i = threadIdx.x; i < nh; i += kStageThreads) tile_gather_halo(a, b, nloc, i, a.tile_halo[h0 + i]);
+    cp_async_wait_all();
+    if (!tile_wait(a, bar, 0)) {
+        for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, 0); it++) {
+        }  // let copies in flight land before the block leaves
+        return;
+    }
+    if (!EXACT) {
+        tile_roots<kStageThreads>(a, b, sq, LC, nloc + nh);
+        __syncthreads();
+    }
+    tile_fluxes<EXACT, kStageThreads>(a, b, sq, fs, LC, FC, nf, c0);
+    __syncthreads();
+    double r2 = 0.0;
+    if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
     if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
-// Dynamic shared memory of tile_kernel for the given maxima.
-inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
-    size_t b = (size_t)smem_cells * 48 + ((40u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
-               kTileCells * 32 + (size_t)max_contrib * kTileCells * 2;
-    b = (b + 15) & ~(size_t)15;
-    b += 5 * (size_t)smem_faces * 8 + 2 * (size_t)smem_cells * 8;
+// ---- persistent, double-buffered (variant 3)
+// One block of kPipeThreads per SM walks tiles blockIdx.x, +gridDim.x, ...  While it evaluates
+// tile i from one buffer, the bulk copies and halo gathers of tile i+1 fill the other, so memory
+// traffic overlaps computation.  Halo indices are read into registers one tile ahead of their use.
+// Shared memory: TileBuf x 2 | fs[5][FC] | sq[2][LC] | mbarrier x 2
+constexpr int kPipeThreads = 512;
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a) {
+    const int n_tiles = a.n_tiles;
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
+    const size_t bb = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
+    const TileBuf buf0 = tile_buf_at(smem_raw, LC, FC, MC), buf1 = tile_buf_at(smem_raw + bb, LC, FC, MC);
+    auto pick = [&](int k) {  // select, not index: keeps the descriptors in registers
+        TileBuf r;
+        r.st = k ? buf1.st : buf0.st;
+        r.rec = k ? buf1.rec : buf0.rec;
+        r.w0 = k ? buf1.w0 : buf0.w0;
+        r.cg = k ? buf1.cg : buf0.cg;
+        r.ct = k ? buf1.ct : buf0.ct;
+        return r;
+    };
+    double *fs = reinterpret_cast<double *>(smem_raw + 2 * bb);
+    double *sq = fs + 5 * FC;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+    const int G = gridDim.x;
+    int tile = blockIdx.x;
+    if (tile >= n_tiles) return;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+    }
+    __syncthreads();
+    auto halo_index = [&](int t) {  // this thread's halo cell of tile t, or -1
+        if (t >= n_tiles) return -1;
+        const int h0 = a.tile_halo_ptr[t], nh = a.tile_halo_ptr[t + 1] - h0;
+        return (int)threadIdx.x < nh ? a.tile_halo[h0 + threadIdx.x] : -1;
+    };
+    // prologue: tile 0 of this block in flight, halo indices of tile 1 on their way
+    if (threadIdx.x == 0) tile_issue_bulk(a, tile, buf0, &bars[0]);
+    {
+        const int h = halo_index(tile);
+        if (h >= 0) tile_gather_halo(a, buf0, min(T, a.n_cells - tile * T), threadIdx.x, h);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    int h_next = halo_index(tile + G);
+
+    for (int i = 0; tile < n_tiles; i++, tile += G) {
+        const int cur = i & 1;
+        const int next = tile + G;
+        // fill the other buffer with the next tile (its previous contents were released at the end of
+        // the last iteration)
+        if (next < n_tiles) {
+            const TileBuf nb = pick(cur ^ 1);
+            if (threadIdx.x == 0) {
+                // the buffer was last read by ordinary loads; order those before the async-proxy writes
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                tile_issue_bulk(a, next, nb, cur ? &bars[0] : &bars[1]);
+            }
+            if (h_next >= 0) tile_gather_halo(a, nb, min(T, a.n_cells - next * T), threadIdx.x, h_next);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        h_next = halo_index(next + G);  // consumed one iteration from now
+        // this tile's data: own cp.async group (all but the newest) and the bulk copies
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        if (!tile_wait(a, cur ? &bars[1] : &bars[0], (uint32_t)((i >> 1) & 1))) {
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            for (int it = 0; it < kWaitLimit && !mbar_try_wait(cur ? &bars[0] : &bars[1], (uint32_t)(((i + 1) >> 1) & 1));
+                 it++) {
+            }
+            return;
+        }
+        const TileBuf b = pick(cur);
+        const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
+        const int nh = a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
+        const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+        if (!EXACT) {
+            tile_roots<kPipeThreads>(a, b, sq, LC, nloc + nh);
+            __syncthreads();
+        }
+        tile_fluxes<EXACT, kPipeThreads>(a, b, sq, fs, LC, FC, nf, c0);
+        __syncthreads();
+        double r2 = 0.0;
+        if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
+        if (a.last_stage && !a.residual_only) block_sum_store<kPipeThreads>(r2, a.partials + tile);
+        __syncthreads();  // buffer cur, fs and sq are free again
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Dynamic shared memory of tile_kernel (buffers = 1) and tile_pipe_kernel (buffers = 2).
+inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib, int buffers = 1) {
+    size_t bb = (size_t)smem_cells * 48 + ((40u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
+                kTileCells * 32 + (size_t)max_contrib * kTileCells * 2;
+    bb = (bb + 15) & ~(size_t)15;
+    size_t b = buffers * bb + 5 * (size_t)smem_faces * 8 + 2 * (size_t)smem_cells * 8;
     b = (b + 15) & ~(size_t)15;
     return b + 16;
 }

@@ -3,16 +3,22 @@
 
 namespace e3d {
 
-// Dynamic shared memory the tile kernel may use (set once per process before launches).
-void prepare_tile_fast(size_t smem_bytes) {
+// Dynamic shared memory the tile kernels may use (set before their first launch).
+void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     cudaFuncSetAttribute(tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (pipe_smem_bytes)
+        cudaFuncSetAttribute(tile_pipe_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pipe_smem_bytes);
 }
 
 // variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;
-// 2: face-tile kernel
+// 2: face tiles, one block per tile; 3: face tiles, persistent and double-buffered
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
-    if (variant == 2) {
+    if (variant == 3) {
+        const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, 2);
+        tile_pipe_kernel<false><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
+    } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 1) {

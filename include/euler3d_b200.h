@@ -179,7 +179,8 @@ typedef struct e3d_run_params {
 	int32_t profile_stages;           /* 1: launch directly and time every stage kernel with CUDA
 	                                     events (stats.stage_ms); 0: CUDA graphs */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
-	                                     register budgets; 3: face tiles (kept for later runs) */
+	                                     register budgets; 3: face tiles; 4: persistent double-buffered
+	                                     face tiles (kept for later runs) */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {

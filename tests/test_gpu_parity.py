@@ -42,7 +42,7 @@ def assert_state_equal(gpu, ora, n_cells, ghost_E_rtol=0.0):
             assert diff.size == 0, f"{k}: {diff.size} entries differ, first {diff[:5]}"
 
 
-KERNELS = [_lib.KERNEL_GATHER, _lib.KERNEL_GATHER_B, _lib.KERNEL_TILE]
+KERNELS = [_lib.KERNEL_GATHER, _lib.KERNEL_GATHER_B, _lib.KERNEL_TILE, _lib.KERNEL_TILE_PIPE]
 ORDERINGS = [_lib.ORDER_NATIVE, _lib.ORDER_RCM, _lib.ORDER_SPATIAL]
 
 
@@ -89,7 +89,7 @@ def test_rk_iteration_bitwise(name, kernel):
 
 
 @pytest.mark.parametrize("name", ["c1", "tets", "ogrid"])
-@pytest.mark.parametrize("kernel", [_lib.KERNEL_GATHER, _lib.KERNEL_TILE])
+@pytest.mark.parametrize("kernel", [_lib.KERNEL_GATHER, _lib.KERNEL_TILE, _lib.KERNEL_TILE_PIPE])
 def test_100_iterations(name, kernel):
     """100 iterations from the freestream: exact mode bit for bit, fast mode within 1e-10."""
     fl_exact = CASES[name].flow(precision=_lib.PREC_FP64_EXACT, ordering=_lib.ORDER_SPATIAL)
@@ -230,6 +230,6 @@ def test_autotune_info():
     name = "tets"
     s = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL))
     info = s.info()
-    assert len(info["variant_ms"]) == 3 and 0 <= info["stage_variant"] < 3
+    assert len(info["variant_ms"]) == 4 and 0 <= info["stage_variant"] < 4
     assert all(t > 0 for t in info["variant_ms"])
     assert info["variant_ms"][info["stage_variant"]] == min(info["variant_ms"])
