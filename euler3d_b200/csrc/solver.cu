@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1169,6 +1170,127 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         st.stage_ms = stage_ms;
         st.stage_launches = stage_launches;
         if (stats) *stats = st;
+        if (c.fault) throw Error(E3D_ERR_TIMEOUT, "a bounded device wait gave up (asynchronous copy did not complete)");
+        if (c.nonfinite)
+            throw Error(E3D_ERR_NONFINITE, "density residual became NaN/Inf at iteration " + std::to_string(c.it));
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free run.  The RMS partials and the RMS history of e3d_solver_run_noalloc live in this
+// file-scope device array instead of handle buffers, and the iterations are launched directly
+// (instantiating a CUDA graph allocates), so the call allocates no memory.  The array is 1 MiB,
+// exists on every device that loads the library until the process exits, and is shared by every
+// call: calls that overlap on the GPU race on it.
+constexpr int kNoAllocMaxBlocks = 65536;  // RMS partials -> at most 65536 x 256 = 16,777,216 cells
+constexpr int kNoAllocMaxIter = 65536;    // RMS history entries -> at most 65536 iterations per call
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + kNoAllocMaxIter];
+
+namespace {
+std::mutex g_noalloc_mutex;
+double *g_noalloc_ptr[64] = {};  // device address of g_noalloc_scratch, per device ordinal
+}  // namespace
+
+// Device address of the scratch array on the current device.  Host code may not use the symbol's
+// name as a pointer (it names the host-side stand-in), so the address is looked up once per device
+// with that device current, on the first call made on it.
+static double *noalloc_scratch(int device) {
+    if (device < 0 || device >= 64) throw Error(E3D_ERR_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        double *p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (err != cudaSuccess || !p)
+            throw Error(E3D_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-alloc scratch failed: ") +
+                                          cudaGetErrorString(err));
+        g_noalloc_ptr[device] = p;
+    }
+    return g_noalloc_ptr[device];
+}
+
+e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, e3d_run_stats *stats,
+                                  double *rms_history, int32_t history_capacity) {
+    return guarded([&] {
+        if (!solver || !rp) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        Solver *S = as_solver(solver);
+        E3D_CUDA(cudaSetDevice(S->device));
+        if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
+        const int max_iter = std::max(rp->max_iter, 0);
+        if (max_iter > kNoAllocMaxIter)
+            throw Error(E3D_ERR_INVALID_ARG, "max_iter " + std::to_string(max_iter) + " exceeds the no-alloc limit of " +
+                                                 std::to_string(kNoAllocMaxIter) + " iterations per call");
+        if (S->n_blocks > kNoAllocMaxBlocks)
+            throw Error(E3D_ERR_INVALID_ARG, "mesh of " + std::to_string(S->N) + " cells exceeds the no-alloc limit of " +
+                                                 std::to_string(kNoAllocMaxBlocks * kStageThreads) + " cells");
+        if (rp->stage_kernel != 0) throw Error(E3D_ERR_INVALID_ARG, "the no-alloc run uses the handle's stage kernel");
+        double *partials = noalloc_scratch(S->device);
+        double *hist = partials + kNoAllocMaxBlocks;
+        // the history region starts cleared, so no entry of an earlier call can be read back
+        E3D_CUDA(cudaMemsetAsync(hist, 0, (size_t)std::max(max_iter, 1) * sizeof(double), S->stream));
+        Control init{};
+        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+        init.minit_valid = S->ctl_host->minit_valid;
+        init.max_iter = max_iter;
+        init.sampling = rp->sampling;
+        init.hist_cap = kNoAllocMaxIter;
+        init.min_res = rp->min_residual;
+        init.min_aero = rp->min_aerocoeff_error;
+        init.done = max_iter == 0;
+        std::memcpy(S->ctl_host, &init, sizeof init);
+        E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
+        if (S->cur != 0) {
+            E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
+                                     cudaMemcpyDeviceToDevice, S->stream));
+            S->cur = 0;
+        }
+        static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+        const int every = rp->check_every > 0 ? rp->check_every : 32;
+        int64_t launches = 0;
+        E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
+        int b = 0;
+        for (int it = 0; it < max_iter; it++) {
+            for (int st_i = 0; st_i < 5; st_i++) {
+                StageArgs a = S->stage_args(b, alphas[st_i], st_i == 0, st_i == 4);
+                a.partials = partials;
+                S->launch_stage(a);
+                b = 1 - b;
+            }
+            finalize_kernel<<<1, kReduceThreads, 0, S->stream>>>(partials, S->n_blocks, (double)S->N, hist, S->ctl);
+            coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
+            E3D_CUDA(cudaGetLastError());
+            launches += 7;
+            if ((it + 1) % every == 0 || it + 1 == max_iter) {
+                E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+                E3D_CUDA(cudaStreamSynchronize(S->stream));
+                if (S->ctl_host->done) break;
+            }
+        }
+        E3D_CUDA(cudaEventRecord(S->ev1, S->stream));
+        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
+        E3D_CUDA(cudaStreamSynchronize(S->stream));
+        float ms = 0.f;
+        E3D_CUDA(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+        const Control &c = *S->ctl_host;
+        S->cur = c.n_rms & 1;
+        e3d_run_stats st{};
+        st.iterations = c.it;
+        st.stop_reason = c.stop_reason;
+        st.n_rms = c.n_rms;
+        st.last_rms = c.last_rms;
+        st.cl = c.cl;
+        st.cd = c.cd;
+        st.cm = c.cm;
+        for (int k = 0; k < 3; k++) {
+            st.force[k] = c.force[k];
+            st.moment[k] = c.moment[k];
+        }
+        st.device_ms = ms;
+        st.kernel_launches = launches;
+        if (stats) *stats = st;
+        if (rms_history && history_capacity > 0 && c.n_rms > 0)
+            E3D_CUDA(cudaMemcpy(rms_history, hist, std::min(c.n_rms, history_capacity) * sizeof(double),
+                                cudaMemcpyDeviceToHost));
         if (c.fault) throw Error(E3D_ERR_TIMEOUT, "a bounded device wait gave up (asynchronous copy did not complete)");
         if (c.nonfinite)
             throw Error(E3D_ERR_NONFINITE, "density residual became NaN/Inf at iteration " + std::to_string(c.it));

@@ -237,6 +237,21 @@ class EulerSolver:
         check(status)
         return stats
 
+    def run_noalloc(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0,
+                    min_aerocoeff_error: float = 0.0, check_every: int = 0):
+        """``e3d_solver_run_noalloc``: the same iterations as :meth:`run` without any device allocation
+        (scratch in a fixed 1 MiB device array; at most 65,536 iterations per call).  Returns
+        (stats, density RMS of every iteration)."""
+        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, 0, 0)
+        st = _lib.RunStats()
+        hist = np.zeros(max(max_iter, 1))
+        status = _lib.load().e3d_solver_run_noalloc(self._h, C.byref(rp), C.byref(st), _dp(hist), hist.size)
+        check(status)
+        stats = {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,
+                 "last_rms": st.last_rms, "cl": st.cl, "cd": st.cd, "cm": st.cm, "force": list(st.force),
+                 "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches}
+        return stats, hist[: st.n_rms].copy()
+
     def rms_history(self) -> np.ndarray:
         n = C.c_int32()
         check(_lib.load().e3d_solver_rms_history(self._h, None, 0, C.byref(n)))

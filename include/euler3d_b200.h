@@ -200,6 +200,21 @@ typedef struct e3d_run_stats {
  * current device state until MAX_ITER, the residual test or the coefficient test stops it. */
 e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *params, e3d_run_stats *stats);
 
+/* e3d_solver_run for callers that must not allocate device memory once set-up is done: a serving
+ * loop that runs inside a fixed, pre-reserved memory budget, or code running where the CUDA
+ * allocator may not be called.  e3d_solver_run itself may allocate (its history buffer grows with
+ * max_iter and it instantiates CUDA graphs); this call allocates nothing.  It computes the same
+ * iterations with the same kernels, launched directly, and keeps its scratch (the per-block RMS
+ * partial sums and the RMS history) in one 1 MiB file-scope device array that every device loading
+ * the library holds until the process exits.  Limits: at most 16,777,216 cells and 65,536
+ * iterations per call; larger requests fail with E3D_ERR_INVALID_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  All calls share the array, so calls that overlap on the GPU race on it.  The
+ * density RMS of every iteration run is copied to rms_history (up to history_capacity entries;
+ * NULL skips it).  params->stage_kernel must be 0.  No counterpart in the reference. */
+e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *params, e3d_run_stats *stats,
+                                  double *rms_history, int32_t history_capacity);
+
 /* Density RMS of every iteration of the last e3d_solver_run (the residuals.dat column). */
 e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count);
 
