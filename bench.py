@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=128, help="hexahedra per box edge (6 tets each)")
-    ap.add_argument("--precision", choices=["fp64", "fp64_exact"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "fp64_exact", "fp32"], default="fp64")
     ap.add_argument("--ordering", choices=["spatial", "rcm", "native"], default="spatial")
     ap.add_argument("--kernel", type=int, default=0, help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined face tiles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -53,12 +53,14 @@ def parse():
     return ap.parse_args()
 
 
-def algorithmic_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
-    """FP64 bytes per cell-stage, each array counted once with ideal gather reuse:
-    160 + 40 f_c (f_c = faces per cell): read W, read U0, write W (3 x 40 B), 1/5 of writing U0
-    (8 B), volume (8 B), sum|S| (24 B); per face 2 x int32 + (nx, ny, nz, S) x 8 B."""
+def algorithmic_bytes_per_cell_stage(n_cells: int, n_faces: int, fp32: bool = False) -> float:
+    """Bytes per cell-stage, each array counted once with ideal gather reuse (f_c = faces per cell).
+    FP64: 160 + 40 f_c -- read W, read U0, write W (3 x 40 B), 1/5 of writing U0 (8 B), volume
+    (8 B), sum|S| (24 B); per face 2 x int32 + (nx, ny, nz, S) x 8 B.
+    FP32 flux / FP64 state: 104 + 24 f_c -- 5 x 4 B primitives read and written, U0 read in double,
+    float volume and sum|S|; per face 2 x int32 + 4 x 4 B."""
     fc = n_faces / n_cells
-    return 160.0 + 40.0 * fc
+    return (104.0 + 24.0 * fc) if fp32 else (160.0 + 40.0 * fc)
 
 
 def measured_peaks():
@@ -159,7 +161,7 @@ def run_ours(args, rank, world, local_rank):
     arrays = Mesh.from_raw(raw).arrays()
     del raw
     n_cells, n_faces = int(arrays["n_cells"]), int(arrays["n_faces"])
-    prec = _lib.PREC_FP64 if args.precision == "fp64" else _lib.PREC_FP64_EXACT
+    prec = {"fp64": _lib.PREC_FP64, "fp64_exact": _lib.PREC_FP64_EXACT, "fp32": _lib.PREC_FP32_FLUX}[args.precision]
     order = {"spatial": _lib.ORDER_SPATIAL, "rcm": _lib.ORDER_RCM, "native": _lib.ORDER_NATIVE}[args.ordering]
     flow = FlowConfig(mach=0.6, aoa=0.0, cfl=1.0, precision=prec, ordering=order, device=local_rank)
     stream = torch.cuda.Stream(device=local_rank)
@@ -200,10 +202,10 @@ def run_ours(args, rank, world, local_rank):
     # ---- stage-kernel duration for the roofline (direct launches, event pair per launch)
     prof = solver.run(max(K // 5, 4), profile_stages=True)
     stage_ms = prof["stage_ms"] / prof["stage_launches"]
-    bytes_per_cell = algorithmic_bytes_per_cell_stage(n_cells, n_faces)
+    bytes_per_cell = algorithmic_bytes_per_cell_stage(n_cells, n_faces, fp32=args.precision == "fp32")
     achieved = bytes_per_cell * n_cells / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    tr = profiled_traffic()
+    tr = profiled_traffic() if args.precision != "fp32" else None
 
     # ---- end to end through the C ABI with host buffers
     e2e = None
@@ -249,15 +251,16 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f32 flux / f64 state" if args.precision == "fp32" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cells": n_cells, "faces": n_faces, "faces_per_cell": n_faces / n_cells,
                    "precision": args.precision, "ordering": args.ordering,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>",
-                                "tile_pipe_kernel<false>"][solver.info()["stage_variant"]],
+                     "kernel": (["-", "-", "tile_kernel_f32<2>", "tile_kernel_f32<3>"] if args.precision == "fp32" else
+                                ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>",
+                                 "tile_pipe_kernel<false>"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "autotune": solver.info()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,

@@ -27,6 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 SOURCES = [
     ("stage_exact.cu", ["-fmad=false"]),
     ("stage_fast.cu", ["-fmad=true"]),
+    ("stage_f32.cu", ["-fmad=true"]),
     ("solver.cu", ["-fmad=false"]),
     ("capi.cpp", []),
     ("mesh_prep.cpp", []),

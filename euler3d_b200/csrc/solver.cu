@@ -16,6 +16,7 @@
 #include "common.hpp"
 #include "euler3d_b200.h"
 #include "stage.cuh"
+#include "stage_f32.cuh"
 
 namespace e3d {
 
@@ -23,6 +24,8 @@ void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant);
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
+void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
+void prepare_tile_f32(size_t smem_bytes);
 constexpr int kStageVariants = 4;  // gather (two register budgets), face tiles, pipelined face tiles
 
 constexpr int kReduceThreads = 256;
@@ -78,6 +81,9 @@ struct CoeffArgs {
     const double *__restrict__ svec;    // 3 per wall face: full face normal
     const double *__restrict__ center;  // 3 per wall face: face centre
     const double2 *__restrict__ q;
+    const double *__restrict__ w0;      // FP32_FLUX mode: pressure from the double conservative state
+    int w0_stride;
+    double gamma;
     double p_inf, cp_factor, cref, sref, ref[3];
     int axis[3], sign[3];
     Control *ctl;
@@ -85,6 +91,13 @@ struct CoeffArgs {
     int sequential;                     // 1: sum in the reference's wall order (FP64_EXACT)
     double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
 };
+
+__device__ __forceinline__ double wall_pressure(const CoeffArgs &a, int c) {
+    if (!a.w0) return a.q[3 * c + 2].x;
+    const size_t st = (size_t)a.w0_stride;
+    const double rho = a.w0[c], mu = a.w0[st + c], mv = a.w0[2 * st + c], mw = a.w0[3 * st + c];
+    return (a.gamma - 1.0) * (a.w0[4 * st + c] - 0.5 * (mu * mu + mv * mv + mw * mw) / rho);
+}
 
 // AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52): face terms in parallel, summed
 // by one thread in the reference's wall order so the sums are the reference's; then
@@ -99,7 +112,7 @@ __global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
         for (int base = 0; base < a.n_wall; base += kCoeffThreads) {
             int i = base + threadIdx.x;
             if (i < a.n_wall) {
-                double p = a.q[3 * a.cell[i] + 2].x;
+                double p = wall_pressure(a, a.cell[i]);
                 double cp = a.cp_factor * (p - a.p_inf);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
@@ -125,7 +138,7 @@ __global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
         // fixed-shape tree: strided per-thread sums, then a pairwise tree (deterministic)
         double acc[6] = {0, 0, 0, 0, 0, 0};
         for (int i = threadIdx.x; i < a.n_wall; i += kCoeffThreads) {
-            double p = a.q[3 * a.cell[i] + 2].x;
+            double p = wall_pressure(a, a.cell[i]);
             double cp = a.cp_factor * (p - a.p_inf);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -235,6 +248,64 @@ __global__ void store_state_kernel(double *__restrict__ st, int64_t T, int n_cel
     }
 }
 
+// FP32_FLUX mode: reference-ordered FlowField arrays -> float cell records and double W0.
+__global__ void load_state_f32_kernel(const double *__restrict__ st, int64_t T, int n_cells, int n_ghosts,
+                                      const int *__restrict__ new2old, const int *__restrict__ ghost_ref,
+                                      float4 *__restrict__ q32, double *__restrict__ w0, int w0_stride,
+                                      double *__restrict__ ecell, double *__restrict__ minit,
+                                      double *__restrict__ ghost, double gamma) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)w0_stride;
+    if (i < n_cells) {
+        int o = new2old[i];
+        double rho = st[o], u = st[T + o], v = st[2 * T + o], w = st[3 * T + o];
+        double p = st[4 * T + o], E = st[5 * T + o], H = st[6 * T + o], M = st[7 * T + o];
+        make_rec32(q32 + 2 * (size_t)i, rho, u, v, w, p, H, gamma);
+        w0[0 * N + i] = rho;
+        w0[1 * N + i] = u * rho;
+        w0[2 * N + i] = v * rho;
+        w0[3 * N + i] = w * rho;
+        w0[4 * N + i] = E * rho;
+        ecell[i] = E;
+        minit[i] = M;
+    } else if (i < n_cells + n_ghosts) {
+        int g = i - n_cells;
+        int r = ghost_ref[g];
+        for (int k = 0; k < 8; k++) ghost[8 * (size_t)g + k] = st[k * T + r];
+    }
+}
+
+// FP32_FLUX mode: the state is the double conservative W0 (updated at every completed RK step).
+__global__ void store_state_f32_kernel(double *__restrict__ st, int64_t T, int n_cells, int n_ghosts,
+                                       const int *__restrict__ new2old, const int *__restrict__ ghost_ref,
+                                       const double *__restrict__ w0, int w0_stride,
+                                       const double *__restrict__ minit, const double *__restrict__ ghost,
+                                       double gamma, const Control *ctl) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)w0_stride;
+    if (i < n_cells) {
+        int o = new2old[i];
+        double rho = w0[i], u = w0[N + i] / rho, v = w0[2 * N + i] / rho, w = w0[3 * N + i] / rho;
+        double E = w0[4 * N + i] / rho;
+        double q2 = u * u + v * v + w * w;
+        double p = (gamma - 1) * rho * (E - q2 / 2.0);
+        double H = E + p / rho;
+        double M = ctl->minit_valid ? minit[i] : sqrt(gamma * (p / rho)) / sqrt(q2);
+        st[o] = rho;
+        st[T + o] = u;
+        st[2 * T + o] = v;
+        st[3 * T + o] = w;
+        st[4 * T + o] = p;
+        st[5 * T + o] = E;
+        st[6 * T + o] = H;
+        st[7 * T + o] = M;
+    } else if (i < n_cells + n_ghosts) {
+        int g = i - n_cells;
+        int r = ghost_ref[g];
+        for (int k = 0; k < 8; k++) st[k * T + r] = ghost[8 * (size_t)g + k];
+    }
+}
+
 // ------------------------------------------------------------------------------ host handle
 
 template <typename T>
@@ -303,6 +374,11 @@ struct Solver {
     DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell, tile_halo_ptr, tile_halo, tile_face_ptr;
     DevBuf<FaceRec> tile_rec;
     DevBuf<long long> tile_rec_off;
+    bool f32 = false;                  // FP32_FLUX mode
+    DevBuf<float4> q32[2], cgeo32;
+    DevBuf<FaceRec32> tile_rec32;
+    DevBuf<long long> tile_rec32_off;
+    size_t tile32_smem = 0;
     DevBuf<unsigned short> tile_contrib;
     int w0_stride = 0;
     int prefetch_distance = 0;  // tile_kernel L2 prefetch distance: resident blocks on the device
@@ -336,6 +412,11 @@ struct Solver {
         for (auto *b : ib) b->release();
         tile_rec.release();
         tile_rec_off.release();
+        q32[0].release();
+        q32[1].release();
+        cgeo32.release();
+        tile_rec32.release();
+        tile_rec32_off.release();
         tile_contrib.release();
         cf.release();
         fgeo.release();
@@ -355,7 +436,8 @@ struct Solver {
     int64_t device_bytes() const {
         return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
                          tile_face_ptr.n) * 4 + (int64_t)cf.n * 8 + (int64_t)tile_rec.n * 40 + (int64_t)tile_rec_off.n * 8 +
-               (int64_t)tile_contrib.n * 2 +
+               (int64_t)tile_contrib.n * 2 + (int64_t)(q32[0].n + q32[1].n + cgeo32.n) * 16 + (int64_t)tile_rec32.n * 24 +
+               (int64_t)tile_rec32_off.n * 8 +
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
                          hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
@@ -381,6 +463,7 @@ struct Solver {
         a.gamma = prm.gamma;
         a.cfl = prm.cfl;
         a.alpha = alpha;
+        a.scheme = prm.scheme;
         a.first_stage = first;
         a.last_stage = last;
         a.new2old = new2old_d.p;
@@ -398,6 +481,11 @@ struct Solver {
         a.prefetch_distance = prefetch_distance;
         a.n_tiles = n_tiles;
         a.pipe_grid = std::min(n_tiles, n_sm);
+        a.q32in = q32[in_buf].p;
+        a.q32out = q32[1 - in_buf].p;
+        a.tile_rec32 = reinterpret_cast<const char *>(tile_rec32.p);
+        a.tile_rec32_off = tile_rec32_off.p;
+        a.cgeo32 = cgeo32.p;
         return a;
     }
 
@@ -406,7 +494,8 @@ struct Solver {
 
     void launch_stage(const StageArgs &a, int v = -1) {
         if (v < 0) v = variant;
-        if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
+        if (f32) launch_stage_f32(a, stream, v);
+        else if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
         else launch_stage_fast(a, stream, v);
     }
 
@@ -422,13 +511,16 @@ struct Solver {
         a.ghost = ghost_copy.p;
         const int reps = N > 200000 ? 3 : 10;
         float best = 1e30f;
-        if (tiles_ok) {
+        if (f32) {
+            prepare_tile_f32(tile32_smem);
+        } else if (tiles_ok) {
             if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
             else prepare_tile_fast(tile_smem, pipe_smem);
         }
         for (int v = 0; v < kStageVariants; v++) {
             variant_ms[v] = -1.0f;
-            if ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok)) continue;
+            // FP32_FLUX mode has face-tile kernels only: variant 2 and 3 are its two register budgets
+            if (f32 ? v < 2 : ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok))) continue;
             launch_stage(a, v);  // warm
             E3D_CUDA(cudaEventRecord(ev0, stream));
             for (int r = 0; r < reps; r++) launch_stage(a, v);
@@ -467,6 +559,9 @@ struct Solver {
         c.ctl = ctl;
         c.run_mode = run_mode;
         c.sequential = prm.precision == E3D_PREC_FP64_EXACT;
+        c.w0 = f32 ? w0.p : nullptr;
+        c.w0_stride = w0_stride;
+        c.gamma = prm.gamma;
         c.out = out;
         return c;
     }
@@ -633,6 +728,23 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
     S->tile_face_ptr.upload(face_ptr, s);
     S->tile_rec.upload(tface, s);
     S->tile_rec_off.upload(rec_off, s);
+    if (S->prm.precision == E3D_PREC_FP32_FLUX) {  // the same faces as 24-byte records, 16-byte blocks
+        std::vector<FaceRec32> r32;
+        std::vector<long long> off32(n_tiles + 1, 0);
+        r32.reserve(tface.size());
+        for (int t = 0; t < n_tiles; t++) {
+            const size_t f0 = (size_t)(rec_off[t] / (long long)sizeof(FaceRec));
+            for (int j = 0; j < face_ptr[t + 1] - face_ptr[t]; j++) {
+                const FaceRec &f = tface[f0 + j];
+                r32.push_back(FaceRec32{f.code, f.ghost, (float)f.nx, (float)f.ny, (float)f.nz, (float)f.S});
+            }
+            while ((r32.size() * sizeof(FaceRec32)) % 16) r32.push_back(FaceRec32{0, -1, 0, 0, 0, 0});
+            off32[t + 1] = (long long)(r32.size() * sizeof(FaceRec32));
+        }
+        S->tile_rec32.upload(r32, s);
+        S->tile_rec32_off.upload(off32, s);
+        S->tile32_smem = tile32_smem_bytes(max_cells, max_faces, max_contrib);
+    }
     S->tile_contrib.upload(contrib, s);
     S->max_contrib = max_contrib;
     S->smem_cells = max_cells;
@@ -680,9 +792,9 @@ static std::vector<int> spatial_order(const e3d_mesh_desc *d) {
 static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solver *S) {
     check_desc(d);
     if (!p) throw Error(E3D_ERR_INVALID_ARG, "flow parameters are NULL");
-    if (p->precision != E3D_PREC_FP64_EXACT && p->precision != E3D_PREC_FP64)
-        throw Error(E3D_ERR_INVALID_ARG, "precision mode not available in this build");
-    if (p->scheme != E3D_SCHEME_ROE) throw Error(E3D_ERR_INVALID_ARG, "flux scheme not available in this build");
+    if (p->precision != E3D_PREC_FP64_EXACT && p->precision != E3D_PREC_FP64 && p->precision != E3D_PREC_FP32_FLUX)
+        throw Error(E3D_ERR_INVALID_ARG, "unknown precision mode");
+    if (p->scheme != E3D_SCHEME_ROE && p->scheme != E3D_SCHEME_AUSM) throw Error(E3D_ERR_INVALID_ARG, "unknown flux scheme");
     if (p->ordering != E3D_ORDER_NATIVE && p->ordering != E3D_ORDER_RCM && p->ordering != E3D_ORDER_SPATIAL)
         throw Error(E3D_ERR_INVALID_ARG, "unknown cell ordering");
     if (!(p->gamma > 1.0) || !(p->cfl > 0.0) || !(p->mach >= 0.0) || !(p->cref != 0.0) || !(p->sref != 0.0))
@@ -869,8 +981,19 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     S->wall_cell.upload(wcell, s);
     S->wall_svec.upload(wsv, s);
     S->wall_center.upload(wct, s);
-    S->q[0].alloc(3 * (size_t)N);
-    S->q[1].alloc(3 * (size_t)N);
+    S->f32 = p->precision == E3D_PREC_FP32_FLUX;
+    if (S->f32) {
+        if (!S->tiles_ok) throw Error(E3D_ERR_INVALID_ARG, "FP32_FLUX mode needs face tiles this mesh cannot form");
+        S->q32[0].alloc(2 * (size_t)N);
+        S->q32[1].alloc(2 * (size_t)N);
+        std::vector<float4> cg32(N);
+        for (int c = 0; c < N; c++)
+            cg32[c] = make_float4((float)cgeo[c].x, (float)cgeo[c].y, (float)cgeo[c].z, (float)cgeo[c].w);
+        S->cgeo32.upload(cg32, s);
+    } else {
+        S->q[0].alloc(3 * (size_t)N);
+        S->q[1].alloc(3 * (size_t)N);
+    }
     S->w0_stride = (N + 31) / 32 * 32;
     S->w0.alloc(5 * (size_t)S->w0_stride);
     S->ecell.alloc(N);
@@ -897,9 +1020,15 @@ static void upload_state(Solver *S, const double *const *arr) {
         E3D_CUDA(cudaMemcpyAsync(S->staging.p + k * T, arr[k], T * sizeof(double), cudaMemcpyHostToDevice, S->stream));
     }
     int threads = 256, blocks = (int)((T + threads - 1) / threads);
-    load_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
-                                                         S->ghost_ref_d.p, S->q[0].p, S->w0.p, S->w0_stride,
-                                                         S->ecell.p, S->minit.p, S->ghost.p);
+    if (S->f32)
+        load_state_f32_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                                 S->ghost_ref_d.p, S->q32[0].p, S->w0.p,
+                                                                 S->w0_stride, S->ecell.p, S->minit.p, S->ghost.p,
+                                                                 S->prm.gamma);
+    else
+        load_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                             S->ghost_ref_d.p, S->q[0].p, S->w0.p, S->w0_stride,
+                                                             S->ecell.p, S->minit.p, S->ghost.p);
     E3D_CUDA(cudaGetLastError());
     S->cur = 0;
     Control init{};
@@ -999,9 +1128,14 @@ e3d_status e3d_solver_get_state(e3d_solver *solver, double *const state[8]) {
         E3D_CUDA(cudaSetDevice(S->device));
         const int64_t T = S->state_size();
         int threads = 256, blocks = (int)((T + threads - 1) / threads);
-        store_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
-                                                              S->ghost_ref_d.p, S->q[S->cur].p, S->ecell.p,
-                                                              S->minit.p, S->ghost.p, S->prm.gamma, S->ctl);
+        if (S->f32)
+            store_state_f32_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                                      S->ghost_ref_d.p, S->w0.p, S->w0_stride,
+                                                                      S->minit.p, S->ghost.p, S->prm.gamma, S->ctl);
+        else
+            store_state_kernel<<<blocks, threads, 0, S->stream>>>(S->staging.p, T, S->N, S->G, S->new2old_d.p,
+                                                                  S->ghost_ref_d.p, S->q[S->cur].p, S->ecell.p,
+                                                                  S->minit.p, S->ghost.p, S->prm.gamma, S->ctl);
         E3D_CUDA(cudaGetLastError());
         for (int k = 0; k < 8; k++)
             E3D_CUDA(cudaMemcpyAsync(state[k], S->staging.p + k * T, T * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1081,15 +1215,20 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         std::memcpy(S->ctl_host, &init, sizeof init);
         E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
         if (S->cur != 0) {
-            E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
-                                     cudaMemcpyDeviceToDevice, S->stream));
+            if (S->f32)
+                E3D_CUDA(cudaMemcpyAsync(S->q32[0].p, S->q32[1].p, 2 * (size_t)S->N * sizeof(float4),
+                                         cudaMemcpyDeviceToDevice, S->stream));
+            else
+                E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, S->stream));
             S->cur = 0;
         }
         if (rp->stage_kernel > 0) {
             const int v = rp->stage_kernel - 1;
-            if (v >= kStageVariants || (v == 2 && !S->tiles_ok) || (v == 3 && !S->pipe_ok))
-                throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh");
-            if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);
+            if (v >= kStageVariants || (S->f32 ? v < 2 : ((v == 2 && !S->tiles_ok) || (v == 3 && !S->pipe_ok))))
+                throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh and precision");
+            if (S->f32) prepare_tile_f32(S->tile32_smem);
+            else if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);
             else if (v >= 2) prepare_tile_fast(S->tile_smem, S->pipe_smem);
             if (v != S->variant && S->graph) {
                 cudaGraphExecDestroy(S->graph);
@@ -1240,8 +1379,12 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
         std::memcpy(S->ctl_host, &init, sizeof init);
         E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
         if (S->cur != 0) {
-            E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
-                                     cudaMemcpyDeviceToDevice, S->stream));
+            if (S->f32)
+                E3D_CUDA(cudaMemcpyAsync(S->q32[0].p, S->q32[1].p, 2 * (size_t)S->N * sizeof(float4),
+                                         cudaMemcpyDeviceToDevice, S->stream));
+            else
+                E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, S->stream));
             S->cur = 0;
         }
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};

@@ -64,6 +64,7 @@ struct StageArgs {
     Control *ctl;
     Freestream fs;
     double gamma, cfl, alpha;
+    int scheme;                      // E3D_SCHEME_ROE or E3D_SCHEME_AUSM (uniform: no divergence)
     int first_stage;                 // stage 1 of an iteration (may read the loaded interior Mach)
     int last_stage;                  // stage 5: write W0/E for the next step and the RMS partials
     int residual_only;               // e3d_solver_residual: write R and dt, leave the state
@@ -86,6 +87,13 @@ struct StageArgs {
     int prefetch_distance;           // tile_kernel: tiles ahead whose data each block prefetches into L2
     int n_tiles;                     // tiles of the mesh
     int pipe_grid;                   // tile_pipe_kernel: persistent blocks (one per SM)
+    // FP32_FLUX mode: float cell records (rho,u,v,w | p,H,sqrt(rho),rsqrt(gamma p rho)), float
+    // face records and float cell geometry; W0 stays double
+    const float4 *__restrict__ q32in;
+    float4 *__restrict__ q32out;
+    const char *__restrict__ tile_rec32;
+    const long long *__restrict__ tile_rec32_off;
+    const float4 *__restrict__ cgeo32;
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -96,6 +104,14 @@ struct FaceRec {
     double nx, ny, nz, S;
 };
 static_assert(sizeof(FaceRec) == 40, "FaceRec layout");
+
+// FP32_FLUX mode face record.
+struct FaceRec32 {
+    int code;
+    int ghost;
+    float nx, ny, nz, S;
+};
+static_assert(sizeof(FaceRec32) == 24, "FaceRec32 layout");
 
 struct Prim {
     double rho, u, v, w, p, H;
@@ -248,6 +264,65 @@ __device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl
     F[3] = 0.5 * (mL * L.w + mR * R.w + (L.p + R.p) * nz - (asum * wt + d51 * nz + a3 * (dw - dV * nz)));
     F[4] = 0.5 * (mL * L.H + mR * R.H -
                   (a15 * ht + d51 * Vt + a2 * (0.5 * q2t) + a3 * (ut * du + vt * dv + wt * dw - Vt * dV)));
+}
+
+// ------------------------------------------------------------------------------ AUSM flux
+// AUSM of Liou & Steffen (J. Comput. Phys. 107, 23-39, 1993).  Exact: the oracle's operation order
+// (oracle/e3d_oracle.c ausm_lr).  Fast: sound speeds from rsqrt(gamma p rho) (rl, rr from the caller).
+__device__ __forceinline__ void ausm_split(double M, double &mp, double &pp, double &mm, double &pm, bool left) {
+    if (left) {
+        if (fabs(M) <= 1.0) {
+            mp = 0.25 * (M + 1.0) * (M + 1.0);
+            pp = mp * (2.0 - M);
+        } else {
+            mp = 0.5 * (M + fabs(M));
+            pp = M > 0.0 ? 1.0 : 0.0;
+        }
+    } else {
+        if (fabs(M) <= 1.0) {
+            mm = -0.25 * (M - 1.0) * (M - 1.0);
+            pm = -mm * (2.0 + M);
+        } else {
+            mm = 0.5 * (M - fabs(M));
+            pm = M < 0.0 ? 1.0 : 0.0;
+        }
+    }
+}
+
+__device__ __forceinline__ void ausm_tail(const Prim &L, const Prim &R, double cl, double cr, double Vl, double Vr,
+                                          double Ml, double Mr, double nx, double ny, double nz, double F[5]) {
+    double mp = 0, pp = 0, mm = 0, pm = 0;
+    ausm_split(Ml, mp, pp, mm, pm, true);
+    ausm_split(Mr, mp, pp, mm, pm, false);
+    (void)Vl;
+    (void)Vr;
+    double mi = mp + mm;
+    double pi = pp * L.p + pm * R.p;
+    double ml = mi > 0.0 ? mi : 0.0, mr = mi < 0.0 ? mi : 0.0;
+    double al = ml * (L.rho * cl), ar = mr * (R.rho * cr);
+    F[0] = al + ar;
+    F[1] = al * L.u + ar * R.u + pi * nx;
+    F[2] = al * L.v + ar * R.v + pi * ny;
+    F[3] = al * L.w + ar * R.w + pi * nz;
+    F[4] = al * L.H + ar * R.H;
+}
+
+__device__ __forceinline__ void ausm_exact(const Prim &L, const Prim &R, double nx, double ny, double nz, double g,
+                                           double F[5]) {
+    double cl = sqrt(g * L.p / L.rho);
+    double cr = sqrt(g * R.p / R.rho);
+    double Vl = L.u * nx + L.v * ny + L.w * nz;
+    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    ausm_tail(L, R, cl, cr, Vl, Vr, Vl / cl, Vr / cr, nx, ny, nz, F);
+}
+
+__device__ __forceinline__ void ausm_fast(const Prim &L, const Prim &R, double rl, double rr, double nx, double ny,
+                                          double nz, double g, double F[5]) {
+    // c = gamma p / sqrt(gamma p rho); 1/c = rho / sqrt(gamma p rho)
+    double cl = g * L.p * rl, cr = g * R.p * rr;
+    double Vl = L.u * nx + L.v * ny + L.w * nz;
+    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    ausm_tail(L, R, cl, cr, Vl, Vr, Vl * (L.rho * rl), Vr * (R.rho * rr), nx, ny, nz, F);
 }
 
 // ------------------------------------------------------------------------------ ghost states
@@ -486,7 +561,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
             Prim fl, fr;
             double sS = fg.w;
             bool roe = true;
-            double s_l = s_me, s_r = s_me, r_l = r_me;
+            double s_l = s_me, s_r = s_me, r_l = r_me, r_nb = r_me;
             if (tag <= TAG_RIGHT) {
                 const Prim nb = load_prim(a.qin, idx);
                 const bool left = tag == TAG_LEFT;
@@ -495,9 +570,10 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
                 sS = left ? fg.w : -fg.w;
                 if (!EXACT) {
                     double s_nb = nb.rho * rsqrt_nr(nb.rho);
+                    r_nb = rsqrt_nr(g * nb.p * nb.rho);
                     s_l = left ? s_me : s_nb;
                     s_r = left ? s_nb : s_me;
-                    r_l = left ? r_me : rsqrt_nr(g * nb.p * nb.rho);
+                    r_l = left ? r_me : r_nb;
                 }
             } else {
                 Prim gs;
@@ -506,8 +582,13 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
                 fr = gs;  // symmetry ghost: rho and p are the cell's, so s_r = s_me
             }
             if (roe) {
-                if (EXACT) roe_exact(fl, fr, fg.x, fg.y, fg.z, g, F);
-                else roe_fast(fl, fr, s_l, s_r, r_l, fg.x, fg.y, fg.z, g, F);
+                if (a.scheme == 1) {
+                    if (EXACT) ausm_exact(fl, fr, fg.x, fg.y, fg.z, g, F);
+                    else ausm_fast(fl, fr, r_l, tag == TAG_LEFT ? r_nb : r_me, fg.x, fg.y, fg.z, g, F);
+                } else {
+                    if (EXACT) roe_exact(fl, fr, fg.x, fg.y, fg.z, g, F);
+                    else roe_fast(fl, fr, s_l, s_r, r_l, fg.x, fg.y, fg.z, g, F);
+                }
             }
 #pragma unroll
             for (int k = 0; k < 5; k++) R[k] += F[k] * sS;
@@ -661,14 +742,24 @@ __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b
         double F[5];
         if (tag == TAG_LEFT) {
             const Prim R = tile_prim(b.st, r);
-            if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
-            else roe_fast(L, R, sq[l], sq[r], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+            if (a.scheme == 1) {
+                if (EXACT) ausm_exact(L, R, fg.x, fg.y, fg.z, g, F);
+                else ausm_fast(L, R, sq[LC + l], sq[LC + r], fg.x, fg.y, fg.z, g, F);
+            } else {
+                if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
+                else roe_fast(L, R, sq[l], sq[r], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+            }
         } else {
             Prim gs;
             double *gp = a.ghost + 8 * (size_t)fr.ghost;
             if (boundary_face(a, tag, gp, c0 + l, L, fg, F, gs)) {
-                if (EXACT) roe_exact(L, gs, fg.x, fg.y, fg.z, g, F);
-                else roe_fast(L, gs, sq[l], sq[l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                if (a.scheme == 1) {
+                    if (EXACT) ausm_exact(L, gs, fg.x, fg.y, fg.z, g, F);
+                    else ausm_fast(L, gs, sq[LC + l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                } else {
+                    if (EXACT) roe_exact(L, gs, fg.x, fg.y, fg.z, g, F);
+                    else roe_fast(L, gs, sq[l], sq[l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                }
             }
         }
 #pragma unroll

@@ -1,0 +1,257 @@
+// FP32_FLUX stage kernel: fluxes, face states and the time step in single precision; the
+// conservative state W0, the residual sums, the Runge-Kutta update and every reduction in double.
+//
+// Same face-tile scheme as tile_kernel (stage.cuh): one block per tile of kTileCells Morton-ordered
+// cells, bulk copies of the tile's contiguous data plus cp.async gathers of its halo onto one
+// mbarrier, each face evaluated once, each cell summing its faces' F*S in ascending reference face
+// id (deterministic).  Cell records are 32 bytes (two float4), face records 24 bytes, so a tile's
+// staging is about half the double-precision one and three blocks fit on an SM.
+#pragma once
+#include "stage.cuh"
+
+namespace e3d {
+
+struct PrimF {
+    float rho, u, v, w, p, H, s, r;  // s = sqrt(rho), r = rsqrt(gamma p rho)
+};
+
+__device__ __forceinline__ float rcp_f(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rsqrt_f(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Cell record of a double-precision state (written by the update and by the state loader).
+__device__ __forceinline__ void make_rec32(float4 *dst, double rho, double u, double v, double w, double p, double H,
+                                           double g) {
+    const float fr = (float)rho, fp = (float)p;
+    dst[0] = make_float4(fr, (float)u, (float)v, (float)w);
+    dst[1] = make_float4(fp, (float)H, fr * rsqrt_f(fr), rsqrt_f((float)g * fp * fr));
+}
+
+// Roe flux with Harten's fix (Solver::Roe, src/solver/ConvectiveFluxesSchemes.cpp:10-165) in single
+// precision, written as F = (F_L + F_R - sum_k a_k r_k) / 2 like roe_fast.
+__device__ __forceinline__ void roe_f32(const PrimF &L, const PrimF &R, float nx, float ny, float nz, float g,
+                                        float F[5]) {
+    const float inv = rcp_f(L.s + R.s);
+    const float wl = L.s * inv, wr = R.s * inv;
+    const float ut = L.u * wl + R.u * wr, vt = L.v * wl + R.v * wr, wt = L.w * wl + R.w * wr;
+    const float ht = L.H * wl + R.H * wr;
+    const float rt = L.s * R.s;
+    const float q2t = ut * ut + vt * vt + wt * wt;
+    const float c2 = (g - 1.0f) * (ht - 0.5f * q2t);
+    const float rc = rsqrt_f(c2);
+    const float ct = c2 * rc, ic2 = rc * rc;
+    const float Vt = ut * nx + vt * ny + wt * nz;
+    const float Vl = L.u * nx + L.v * ny + L.w * nz;
+    const float Vr = R.u * nx + R.v * ny + R.w * nz;
+    const float drho = R.rho - L.rho, dp = R.p - L.p, dV = Vr - Vl;
+    const float du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+    const float delta = (1.0f / 15.0f) * (g * L.p * L.r);
+    float lam1 = fabsf(Vt - ct), lam5 = fabsf(Vt + ct);
+    if (!(lam1 > delta) || !(lam5 > delta)) {
+        const float h = 7.5f * (L.rho * L.r);
+        if (!(lam1 > delta)) lam1 = (lam1 * lam1 + delta * delta) * h;
+        if (!(lam5 > delta)) lam5 = (lam5 * lam5 + delta * delta) * h;
+    }
+    const float rcdv = rt * ct * dV;
+    const float a1 = 0.5f * lam1 * (dp - rcdv) * ic2;
+    const float a5 = 0.5f * lam5 * (dp + rcdv) * ic2;
+    const float aV = fabsf(Vt);
+    const float a2 = aV * (drho - dp * ic2);
+    const float a3 = aV * rt;
+    const float a15 = a1 + a5, d51 = (a5 - a1) * ct, asum = a15 + a2;
+    const float mL = L.rho * Vl, mR = R.rho * Vr, ps = L.p + R.p;
+    F[0] = 0.5f * (mL + mR - asum);
+    F[1] = 0.5f * (mL * L.u + mR * R.u + ps * nx - (asum * ut + d51 * nx + a3 * (du - dV * nx)));
+    F[2] = 0.5f * (mL * L.v + mR * R.v + ps * ny - (asum * vt + d51 * ny + a3 * (dv - dV * ny)));
+    F[3] = 0.5f * (mL * L.w + mR * R.w + ps * nz - (asum * wt + d51 * nz + a3 * (dw - dV * nz)));
+    F[4] = 0.5f * (mL * L.H + mR * R.H - (a15 * ht + d51 * Vt + a2 * (0.5f * q2t) + a3 * (ut * du + vt * dv + wt * dw - Vt * dV)));
+}
+
+// AUSM (Liou & Steffen 1993) in single precision; c = gamma p r, M = V rho r.
+__device__ __forceinline__ void ausm_f32(const PrimF &L, const PrimF &R, float nx, float ny, float nz, float g,
+                                         float F[5]) {
+    const float cl = g * L.p * L.r, cr = g * R.p * R.r;
+    const float Vl = L.u * nx + L.v * ny + L.w * nz, Vr = R.u * nx + R.v * ny + R.w * nz;
+    const float Ml = Vl * (L.rho * L.r), Mr = Vr * (R.rho * R.r);
+    float mp, pp, mm, pm;
+    if (fabsf(Ml) <= 1.0f) {
+        mp = 0.25f * (Ml + 1.0f) * (Ml + 1.0f);
+        pp = mp * (2.0f - Ml);
+    } else {
+        mp = 0.5f * (Ml + fabsf(Ml));
+        pp = Ml > 0.0f ? 1.0f : 0.0f;
+    }
+    if (fabsf(Mr) <= 1.0f) {
+        mm = -0.25f * (Mr - 1.0f) * (Mr - 1.0f);
+        pm = -mm * (2.0f + Mr);
+    } else {
+        mm = 0.5f * (Mr - fabsf(Mr));
+        pm = Mr < 0.0f ? 1.0f : 0.0f;
+    }
+    const float mi = mp + mm, pi = pp * L.p + pm * R.p;
+    const float al = fmaxf(mi, 0.0f) * (L.rho * cl), ar = fminf(mi, 0.0f) * (R.rho * cr);
+    F[0] = al + ar;
+    F[1] = al * L.u + ar * R.u + pi * nx;
+    F[2] = al * L.v + ar * R.v + pi * ny;
+    F[3] = al * L.w + ar * R.w + pi * nz;
+    F[4] = al * L.H + ar * R.H;
+}
+
+__device__ __forceinline__ PrimF prim32(const float4 *st, int i) {
+    const float4 a = st[2 * i], b = st[2 * i + 1];
+    return PrimF{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+}
+
+// Shared memory: st[LC] 32-byte records | rec[FC] | w0[5][T] (double) | cg[T] | ct[MC][T] | fs[5][FC] (float)
+// | mbarrier
+inline size_t tile32_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
+    size_t b = (size_t)smem_cells * 32 + ((24u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
+               kTileCells * 16 + (size_t)max_contrib * kTileCells * 2;
+    b = (b + 15) & ~(size_t)15;
+    b += 5 * (size_t)smem_faces * 4;
+    b = (b + 15) & ~(size_t)15;
+    return b + 16;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
+    size_t off = 0;
+    float4 *st = reinterpret_cast<float4 *>(smem_raw + off);
+    off += (size_t)LC * 32;
+    FaceRec32 *rec = reinterpret_cast<FaceRec32 *>(smem_raw + off);
+    off += round16(24u * FC);
+    double *w0s = reinterpret_cast<double *>(smem_raw + off);
+    off += 5 * T * 8;
+    float4 *cgs = reinterpret_cast<float4 *>(smem_raw + off);
+    off += T * 16;
+    unsigned short *cts = reinterpret_cast<unsigned short *>(smem_raw + off);
+    off += (size_t)MC * T * 2;
+    off = (off + 15) & ~(size_t)15;
+    float *fs = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)5 * FC * 4;
+    off = (off + 15) & ~(size_t)15;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
+    const int tile = blockIdx.x, c0 = tile * T;
+    const int nloc = min(T, a.n_cells - c0);
+    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
+    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+    const float gf = (float)a.gamma;
+
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t b_state = (uint32_t)nloc * 32u;
+        const uint32_t b_rec = round16(24u * (uint32_t)nf);
+        const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
+        const uint32_t b_cg = (uint32_t)nloc * 16u;
+        const uint32_t b_ct = (uint32_t)MC * T * 2u;
+        mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
+        bulk_g2s(st, a.q32in + 2 * (size_t)c0, b_state, bar);
+        bulk_g2s(rec, a.tile_rec32 + a.tile_rec32_off[tile], b_rec, bar);
+        for (int k = 0; k < 5; k++) bulk_g2s(w0s + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
+        bulk_g2s(cgs, a.cgeo32 + c0, b_cg, bar);
+        bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+    }
+    for (int i = threadIdx.x; i < nh; i += kStageThreads) {
+        const int h = a.tile_halo[h0 + i];
+        cp_async16(st + 2 * (nloc + i), a.q32in + 2 * (size_t)h);
+        cp_async16(st + 2 * (nloc + i) + 1, a.q32in + 2 * (size_t)h + 1);
+    }
+    cp_async_wait_all();
+    if (!tile_wait(a, bar, 0)) {
+        for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, 0); it++) {
+        }
+        return;
+    }
+
+    // one flux per tile face
+    for (int j = threadIdx.x; j < nf; j += kStageThreads) {
+        const FaceRec32 fr = rec[j];
+        const int l = fr.code & ((1 << kTileLocalBits) - 1);
+        const int r = (fr.code >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
+        const int tag = fr.code >> (2 * kTileLocalBits);
+        const PrimF L = prim32(st, l);
+        float F[5];
+        if (tag == TAG_LEFT) {
+            if (a.scheme == 1) ausm_f32(L, prim32(st, r), fr.nx, fr.ny, fr.nz, gf, F);
+            else roe_f32(L, prim32(st, r), fr.nx, fr.ny, fr.nz, gf, F);
+        } else {  // ghost cells are kept in double; their update uses the double boundary code
+            const Prim Ld{L.rho, L.u, L.v, L.w, L.p, L.H};
+            const double4 fg = make_double4(fr.nx, fr.ny, fr.nz, fr.S);
+            double Fd[5];
+            Prim gs;
+            if (boundary_face(a, tag, a.ghost + 8 * (size_t)fr.ghost, c0 + l, Ld, fg, Fd, gs)) {
+                const PrimF G{(float)gs.rho, (float)gs.u, (float)gs.v, (float)gs.w, (float)gs.p, (float)gs.H, L.s, L.r};
+                if (a.scheme == 1) ausm_f32(L, G, fr.nx, fr.ny, fr.nz, gf, F);
+                else roe_f32(L, G, fr.nx, fr.ny, fr.nz, gf, F);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 5; k++) F[k] = (float)Fd[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 5; k++) fs[k * FC + j] = F[k] * fr.S;
+    }
+    __syncthreads();
+
+    double r2 = 0.0;
+    const int i = threadIdx.x;
+    if (i < nloc) {
+        const PrimF me = prim32(st, i);
+        double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        unsigned short e[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) e[k] = k < MC ? cts[k * T + i] : kNoContrib;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            if (e[k] == kNoContrib) break;
+            const int j = e[k] >> 1;
+            const double sg = (e[k] & 1) ? -1.0 : 1.0;
+#pragma unroll
+            for (int q = 0; q < 5; q++) R[q] += sg * (double)fs[q * FC + j];
+        }
+        // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
+        const float4 cg = cgs[i];
+        const float snd = gf * me.p * me.r;
+        const float lam = 0.5f * ((fabsf(me.u) + snd) * cg.x + (fabsf(me.v) + snd) * cg.y + (fabsf(me.w) + snd) * cg.z);
+        const int c = c0 + i;
+        if (a.residual_only) {
+            const int o = a.new2old[c];
+#pragma unroll
+            for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
+            a.dt_out[o] = (double)(a.cfl * cg.w / lam);
+        } else {
+            // W = W0 - alpha dt R / V in double (alpha dt / V = alpha cfl / lambda)
+            const double coef = a.alpha * a.cfl / (double)lam;
+            double W[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) W[k] = w0s[k * T + i] - coef * R[k];
+            const double ir = 1.0 / W[0];
+            const double u = W[1] * ir, v = W[2] * ir, w = W[3] * ir;
+            const double p = (a.gamma - 1.0) * (W[4] - 0.5 * (W[1] * u + W[2] * v + W[3] * w));
+            const double H = (W[4] + p) * ir;
+            make_rec32(a.q32out + 2 * (size_t)c, W[0], u, v, w, p, H, a.gamma);
+            if (a.last_stage) {  // the conservative state carries over exactly in double
+                const size_t sd = (size_t)a.w0_stride;
+#pragma unroll
+                for (int k = 0; k < 5; k++) a.w0[k * sd + c] = W[k];
+                a.ecell[c] = W[4] * ir;
+                r2 = R[0] * R[0];
+            }
+        }
+    }
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+}
+
+}  // namespace e3d

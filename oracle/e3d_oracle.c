@@ -191,6 +191,51 @@ void orc_roe(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, d
 	roe_lr(fl, s, m->face2cell[2 * f], m->face2cell[2 * f + 1], m->face_unit_normal + 3 * (size_t) f, F);
 }
 
+/* AUSM (Liou & Steffen 1993): interface Mach number from the split Mach numbers of both sides,
+ * interface pressure from the split pressures, and the convected quantities rho*c*(1,u,v,w,H) taken
+ * from the upwind side of the interface Mach number. */
+static void ausm_lr(const orc_flow *fl, const orc_state *s, int L, int R, const double *n, double F[5]) {
+	const double g = fl->gamma;
+	double cl = sqrt(g * s->p[L] / s->rho[L]);
+	double cr = sqrt(g * s->p[R] / s->rho[R]);
+	double Vl = s->u[L] * n[0] + s->v[L] * n[1] + s->w[L] * n[2];
+	double Vr = s->u[R] * n[0] + s->v[R] * n[1] + s->w[R] * n[2];
+	double Ml = Vl / cl, Mr = Vr / cr;
+	double mp, pp, mm, pm;
+	if (fabs(Ml) <= 1.0) {
+		mp = 0.25 * (Ml + 1.0) * (Ml + 1.0);
+		pp = mp * (2.0 - Ml);
+	} else {
+		mp = 0.5 * (Ml + fabs(Ml));
+		pp = Ml > 0.0 ? 1.0 : 0.0;
+	}
+	if (fabs(Mr) <= 1.0) {
+		mm = -0.25 * (Mr - 1.0) * (Mr - 1.0);
+		pm = -mm * (2.0 + Mr);
+	} else {
+		mm = 0.5 * (Mr - fabs(Mr));
+		pm = Mr < 0.0 ? 1.0 : 0.0;
+	}
+	double mi = mp + mm;
+	double pi = pp * s->p[L] + pm * s->p[R];
+	double ml = mi > 0.0 ? mi : 0.0, mr = mi < 0.0 ? mi : 0.0;
+	double al = ml * (s->rho[L] * cl), ar = mr * (s->rho[R] * cr);
+	F[0] = al + ar;
+	F[1] = al * s->u[L] + ar * s->u[R] + pi * n[0];
+	F[2] = al * s->v[L] + ar * s->v[R] + pi * n[1];
+	F[3] = al * s->w[L] + ar * s->w[R] + pi * n[2];
+	F[4] = al * s->H[L] + ar * s->H[R];
+}
+
+void orc_ausm(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, double F[5]) {
+	ausm_lr(fl, s, m->face2cell[2 * f], m->face2cell[2 * f + 1], m->face_unit_normal + 3 * (size_t) f, F);
+}
+
+static void face_flux(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, double F[5]) {
+	if (fl->scheme == 1) orc_ausm(m, fl, s, f, F);
+	else orc_roe(m, fl, s, f, F);
+}
+
 /* Solver::Fc, src/solver/ConvectiveFluxesSchemes.cpp:167-187: physical flux of the ghost state. */
 static void ghost_flux(const orc_state *s, int g, const double *n, double V, double F[5]) {
 	double rho = s->rho[g];
@@ -228,7 +273,7 @@ void orc_compute_residual(const orc_mesh *m, const orc_flow *fl, const orc_state
 	double F[5];
 	for (int f = 0; f < m->n_faces_int; f++) {
 		int L = m->face2cell[2 * f], Rc = m->face2cell[2 * f + 1];
-		orc_roe(m, fl, s, f, F);
+		face_flux(m, fl, s, f, F);
 		double S = m->face_area[f];
 		for (int k = 0; k < 5; k++) {
 			double t = F[k] * S;
@@ -249,7 +294,7 @@ void orc_compute_residual(const orc_mesh *m, const orc_flow *fl, const orc_state
 			F[3] = n[2] * s->p[G];
 			F[4] = 0;
 		} else if (contains(sym, m->n_sym, G)) {
-			orc_roe(m, fl, s, f, F);
+			face_flux(m, fl, s, f, F);
 		} else {
 			double V = s->u[G] * n[0] + s->v[G] * n[1] + s->w[G] * n[2];
 			ghost_flux(s, G, n, V, F);

@@ -49,6 +49,7 @@ typedef struct {
 	double rho_inf, p_inf, u_inf, v_inf, w_inf, E_inf, H_inf, M_inf; /* filled by orc_flow_init */
 	double sref, cref, ref_point[3];
 	int cl_axis, cl_sign, cd_axis, cd_sign, cm_axis, cm_sign;
+	int scheme;                     /* 0 Roe (the reference), 1 AUSM (declared, never defined, in the reference) */
 } orc_flow;
 
 typedef struct {                    /* each array holds n_cells + (n_faces - n_faces_int) values */
@@ -84,6 +85,10 @@ void orc_compute_residual(const orc_mesh *m, const orc_flow *fl, const orc_state
 void orc_time_step(const orc_mesh *m, const orc_flow *fl, const orc_state *s, double *dt);
 /* Solver::Roe (src/solver/ConvectiveFluxesSchemes.cpp:10-165) on face f */
 void orc_roe(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, double F[5]);
+/* AUSM of Liou & Steffen (J. Comput. Phys. 107, 23-39, 1993) on face f.  The reference declares
+ * Solver::AUSM (include/solver/ConvectiveFluxesSchemes.h:27-30) but never defines it, so this one is
+ * not pinned to the reference; computeResidual uses it in place of Roe when fl->scheme == 1. */
+void orc_ausm(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, double F[5]);
 /* EulerSolver::RungeKutta (src/solver/EulerSolver.cpp:425-472): R holds the residual of the current
  * state on entry and the stage-5 residual on return; dt is scratch [n_cells]. */
 void orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *R, double *dt);

@@ -42,7 +42,7 @@ class OrcFlow(C.Structure):
                 ("w_inf", C.c_double), ("E_inf", C.c_double), ("H_inf", C.c_double), ("M_inf", C.c_double),
                 ("sref", C.c_double), ("cref", C.c_double), ("ref_point", C.c_double * 3),
                 ("cl_axis", C.c_int), ("cl_sign", C.c_int), ("cd_axis", C.c_int), ("cd_sign", C.c_int),
-                ("cm_axis", C.c_int), ("cm_sign", C.c_int)]
+                ("cm_axis", C.c_int), ("cm_sign", C.c_int), ("scheme", C.c_int)]
 
 
 class OrcState(C.Structure):
@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
         L.orc_compute_residual.argtypes = [M, F, S, _dp]
         L.orc_time_step.argtypes = [M, F, S, _dp]
         L.orc_roe.argtypes = [M, F, S, C.c_int, _dp]
+        L.orc_ausm.argtypes = [M, F, S, C.c_int, _dp]
         L.orc_runge_kutta.argtypes = [M, F, S, _dp, _dp]
         L.orc_rms.argtypes = [M, _dp]
         L.orc_rms.restype = C.c_double
@@ -132,8 +133,9 @@ class Mesh:
 
 
 def flow(mach: float, aoa: float = 0.0, gamma: float = 1.4, cfl: float = 1.5, sref: float = 1.0,
-         cref: float = 1.0, ref_point=(0.25, 0.0, 0.0), cl=(1, 1), cd=(0, 1), cm=(2, 1)) -> OrcFlow:
+         cref: float = 1.0, ref_point=(0.25, 0.0, 0.0), cl=(1, 1), cd=(0, 1), cm=(2, 1), scheme: int = 0) -> OrcFlow:
     f = OrcFlow()
+    f.scheme = scheme
     f.gamma, f.cfl, f.mach, f.aoa_deg = gamma, cfl, mach, aoa
     f.sref, f.cref = sref, cref
     f.ref_point[:] = list(ref_point)
