@@ -11,6 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libeuler3d_b200.so")
 
+ABI_VERSION = 2
 E3D_OK, E3D_ERR_INVALID_ARG, E3D_ERR_OOM, E3D_ERR_NONFINITE, E3D_ERR_TIMEOUT, E3D_ERR_CUDA, E3D_ERR_MESH = range(7)
 SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
@@ -48,7 +49,7 @@ class FlowParams(C.Structure):
 class RunParams(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("sampling", C.c_int32), ("min_residual", C.c_double),
                 ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32),
-                ("stage_kernel", C.c_int32)]
+                ("stage_kernel", C.c_int32), ("min_residual_drop", C.c_double)]
 
 
 class RunStats(C.Structure):
@@ -62,6 +63,12 @@ class SolverInfo(C.Structure):
     _fields_ = [("n_cells", C.c_int32), ("n_ghosts", C.c_int32), ("n_faces", C.c_int32),
                 ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 4),
                 ("device_bytes", C.c_int64)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_members", C.c_int32), ("n_running", C.c_int32), ("n_tiles", C.c_int32),
+                ("graph_builds", C.c_int32), ("member_device_bytes", C.c_int64), ("device_bytes", C.c_int64),
+                ("last_step_ms", C.c_double), ("kernel_launches", C.c_int64)]
 
 
 class E3DError(RuntimeError):
@@ -93,6 +100,14 @@ SIGNATURES = {
     "e3d_solver_run_noalloc": (C.c_int, [C.c_void_p, C.POINTER(RunParams), C.POINTER(RunStats), _dp, C.c_int32]),
     "e3d_solver_residual": (C.c_int, [C.c_void_p, _dp, _dp]),
     "e3d_solver_coefficients": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "e3d_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "e3d_batch_destroy": (None, [C.c_void_p]),
+    "e3d_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunParams)]),
+    "e3d_batch_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "e3d_batch_retire": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(RunStats), C.POINTER(C.c_int),
+                                   C.c_int32, C.POINTER(C.c_int32)]),
+    "e3d_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunStats)]),
+    "e3d_batch_info_get": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
     "e3d_status_string": (C.c_char_p, [C.c_int]),
     "e3d_last_error": (C.c_char_p, []),
     "e3d_abi_version": (C.c_int32, []),
@@ -114,7 +129,7 @@ def load() -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.e3d_abi_version() != 1:
+    if lib.e3d_abi_version() != ABI_VERSION:
         raise ImportError("euler3d_b200 library ABI version mismatch")
     _lib = lib
     return lib

@@ -29,6 +29,7 @@ SOURCES = [
     ("stage_fast.cu", ["-fmad=true"]),
     ("stage_f32.cu", ["-fmad=true"]),
     ("solver.cu", ["-fmad=false"]),
+    ("batch.cu", ["-fmad=false"]),
     ("capi.cpp", []),
     ("mesh_prep.cpp", []),
 ]

@@ -2,8 +2,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "euler3d_b200.h"
 
@@ -27,6 +30,20 @@ inline void cuda_check(cudaError_t err, const char *what) {
 }
 
 #define E3D_CUDA(call) ::e3d::cuda_check((call), #call)
+
+// Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`.  Never
+// lowers it: solvers of different meshes, driven from several host threads, share the kernels.
+inline void raise_smem_limit(const void *func, size_t bytes) {
+    static std::mutex m;
+    static std::map<std::pair<const void *, int>, size_t> limit;
+    int dev = 0;
+    E3D_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(m);
+    size_t &cur = limit[{func, dev}];
+    if (bytes <= cur) return;
+    E3D_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+}
 
 // Runs fn and converts exceptions into an e3d_status plus the thread's last-error message.
 template <typename F>

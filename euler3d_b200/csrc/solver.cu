@@ -15,33 +15,22 @@
 
 #include "common.hpp"
 #include "euler3d_b200.h"
-#include "stage.cuh"
+#include "solver.hpp"
 #include "stage_f32.cuh"
 
 namespace e3d {
 
-void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant);
-void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
-void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
-void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
-void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
-void prepare_tile_f32(size_t smem_bytes);
-constexpr int kStageVariants = 4;  // gather (two register budgets), face tiles, pipelined face tiles
-
-constexpr int kReduceThreads = 256;
-constexpr int kCoeffThreads = 512;
 
 // ------------------------------------------------------------------------------ small kernels
 
 // Sum of the per-block partials in a fixed order, RMS, and the stop tests of
-// EulerSolver::Run (src/solver/EulerSolver.cpp:96-112).
-__global__ void __launch_bounds__(kReduceThreads) finalize_kernel(const double *__restrict__ partials, int n_part,
-                                                                  double n_domain, double *__restrict__ hist,
-                                                                  Control *ctl) {
+// EulerSolver::Run (src/solver/EulerSolver.cpp:96-112).  One block per solver; `sh` is the block's
+// kReduceThreads-entry scratch.
+__device__ __forceinline__ void finalize_body(const FinalizeArgs &f, double *sh) {
+    Control *ctl = f.ctl;
     if (ctl->done) return;
-    __shared__ double sh[kReduceThreads];
     double v = 0.0;
-    for (int i = threadIdx.x; i < n_part; i += kReduceThreads) v += partials[i];
+    for (int i = threadIdx.x; i < f.n_part; i += kReduceThreads) v += f.partials[i];
     sh[threadIdx.x] = v;
     __syncthreads();
     for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
@@ -49,8 +38,9 @@ __global__ void __launch_bounds__(kReduceThreads) finalize_kernel(const double *
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
-    double rms = sqrt(sh[0] / n_domain);
-    if (ctl->n_rms < ctl->hist_cap) hist[ctl->n_rms] = rms;
+    double rms = sqrt(sh[0] / f.n_domain);
+    if (ctl->n_rms < ctl->hist_cap) f.hist[ctl->n_rms] = rms;
+    if (ctl->n_rms == 0) ctl->rms0 = rms;
     ctl->n_rms += 1;
     ctl->last_rms = rms;
     ctl->minit_valid = 0;
@@ -61,7 +51,7 @@ __global__ void __launch_bounds__(kReduceThreads) finalize_kernel(const double *
         ctl->stop_reason = E3D_STOP_MAX_ITER;
         return;
     }
-    if (rms < ctl->min_res) {
+    if (rms < ctl->min_res || (ctl->min_drop > 0.0 && rms < ctl->min_drop * ctl->rms0)) {
         ctl->done = 1;
         ctl->stop_reason = E3D_STOP_RESIDUAL;
         return;
@@ -75,22 +65,19 @@ __global__ void __launch_bounds__(kReduceThreads) finalize_kernel(const double *
     }
 }
 
-struct CoeffArgs {
-    int n_wall;
-    const int *__restrict__ cell;       // device cell of each wall face, reference wall order
-    const double *__restrict__ svec;    // 3 per wall face: full face normal
-    const double *__restrict__ center;  // 3 per wall face: face centre
-    const double2 *__restrict__ q;
-    const double *__restrict__ w0;      // FP32_FLUX mode: pressure from the double conservative state
-    int w0_stride;
-    double gamma;
-    double p_inf, cp_factor, cref, sref, ref[3];
-    int axis[3], sign[3];
-    Control *ctl;
-    int run_mode;                       // 1: sampled inside e3d_solver_run, apply the stop test
-    int sequential;                     // 1: sum in the reference's wall order (FP64_EXACT)
-    double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
-};
+__global__ void __launch_bounds__(kReduceThreads) finalize_kernel(FinalizeArgs f) {
+    __shared__ double sh[kReduceThreads];
+    finalize_body(f, sh);
+}
+
+// Block m: member m of a batch.
+__global__ void __launch_bounds__(kReduceThreads) finalize_batch_kernel(const FinalizeArgs *__restrict__ f,
+                                                                        const int *__restrict__ n_members) {
+    if ((int)blockIdx.x >= *n_members) return;
+    __shared__ double sh[kReduceThreads];
+    const FinalizeArgs a = f[blockIdx.x];
+    finalize_body(a, sh);
+}
 
 __device__ __forceinline__ double wall_pressure(const CoeffArgs &a, int c) {
     if (!a.w0) return a.q[3 * c + 2].x;
@@ -102,10 +89,10 @@ __device__ __forceinline__ double wall_pressure(const CoeffArgs &a, int c) {
 // AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52): face terms in parallel, summed
 // by one thread in the reference's wall order so the sums are the reference's; then
 // EulerSolver::ConvergenceCriteria and the CL/CD/CM selection (src/solver/EulerSolver.cpp:132-152, :253-279).
-__global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
+// One block per solver; `terms` is the block's 6 x kCoeffThreads scratch.
+__device__ __forceinline__ void coeff_body(const CoeffArgs &a, double (*terms)[kCoeffThreads]) {
     Control *ctl = a.ctl;
     if (a.run_mode && (ctl->done || !ctl->sample_now)) return;
-    __shared__ double terms[6][kCoeffThreads];
     double F[3] = {0, 0, 0}, CP[3] = {0, 0, 0};
     if (a.sequential) {
         // the reference's order: one running sum over the wall list
@@ -190,6 +177,42 @@ __global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
         ctl->done = 1;
         ctl->stop_reason = E3D_STOP_MAX_ITER;
     }
+}
+
+__global__ void __launch_bounds__(kCoeffThreads) coeff_kernel(CoeffArgs a) {
+    __shared__ double terms[6][kCoeffThreads];
+    coeff_body(a, terms);
+}
+
+// Block m: member m of a batch, its arguments for the state buffer `parity`.
+__global__ void __launch_bounds__(kCoeffThreads) coeff_batch_kernel(const CoeffArgs *__restrict__ c,
+                                                                    const int *__restrict__ n_members, int parity) {
+    if ((int)blockIdx.x >= *n_members) return;
+    __shared__ double terms[6][kCoeffThreads];
+    const CoeffArgs a = c[2 * blockIdx.x + parity];
+    coeff_body(a, terms);
+}
+
+// Control blocks of a batch's members into one array (read back with one copy).
+__global__ void control_gather_kernel(Control *const *__restrict__ ctl, const int *__restrict__ n_members,
+                                      Control *__restrict__ out) {
+    const int m = blockIdx.x;
+    if (m >= *n_members) return;
+    const int *src = reinterpret_cast<const int *>(ctl[m]);
+    int *dst = reinterpret_cast<int *>(out + m);
+    for (int i = threadIdx.x; i < (int)(sizeof(Control) / 4); i += blockDim.x) dst[i] = src[i];
+}
+
+void launch_finalize(const FinalizeArgs &f, cudaStream_t s) { finalize_kernel<<<1, kReduceThreads, 0, s>>>(f); }
+void launch_coeff(const CoeffArgs &c, cudaStream_t s) { coeff_kernel<<<1, kCoeffThreads, 0, s>>>(c); }
+void launch_finalize_batch(const FinalizeArgs *f, const int *n_members, int grid, cudaStream_t s) {
+    finalize_batch_kernel<<<grid, kReduceThreads, 0, s>>>(f, n_members);
+}
+void launch_coeff_batch(const CoeffArgs *c, const int *n_members, int parity, int grid, cudaStream_t s) {
+    coeff_batch_kernel<<<grid, kCoeffThreads, 0, s>>>(c, n_members, parity);
+}
+void launch_control_gather(Control *const *ctl, const int *n_members, Control *out, int grid, cudaStream_t s) {
+    control_gather_kernel<<<grid, 64, 0, s>>>(ctl, n_members, out);
 }
 
 // Reference-ordered FlowField arrays (staging, 8 x T) -> device layout.
@@ -308,23 +331,6 @@ __global__ void store_state_f32_kernel(double *__restrict__ st, int64_t T, int n
 
 // ------------------------------------------------------------------------------ host handle
 
-template <typename T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    void alloc(size_t count) {
-        n = count;
-        if (count) E3D_CUDA(cudaMalloc(&p, count * sizeof(T)));
-    }
-    void upload(const std::vector<T> &v, cudaStream_t s) {
-        alloc(v.size());
-        if (n) E3D_CUDA(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-    }
-};
 
 // Reverse Cuthill-McKee order of the interior cell graph (each connected component from a
 // minimum-degree start, neighbours visited by increasing degree, whole order reversed).
@@ -358,250 +364,7 @@ static std::vector<int> rcm_order(int n, const std::vector<int> &adj_ptr, const 
     return order;
 }
 
-struct Solver {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int N = 0, G = 0, F = 0, Fint = 0;
-    e3d_flow_params prm{};
-    Freestream fs{};
-    double cp_factor = 0;
-    int n_wall = 0;
-    int n_blocks = 0;
 
-    std::vector<int> new2old, ghost_ref;  // host copies of the maps
-
-    DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell, tile_halo_ptr, tile_halo, tile_face_ptr;
-    DevBuf<FaceRec> tile_rec;
-    DevBuf<long long> tile_rec_off;
-    bool f32 = false;                  // FP32_FLUX mode
-    DevBuf<float4> q32[2], cgeo32;
-    DevBuf<FaceRec32> tile_rec32;
-    DevBuf<long long> tile_rec32_off;
-    size_t tile32_smem = 0;
-    DevBuf<unsigned short> tile_contrib;
-    int w0_stride = 0;
-    int prefetch_distance = 0;  // tile_kernel L2 prefetch distance: resident blocks on the device
-    bool tiles_ok = false, pipe_ok = false;
-    size_t pipe_smem = 0;
-    int n_tiles = 0, n_sm = 0;
-    int max_contrib = 0, smem_cells = 0, smem_faces = 0;
-    size_t tile_smem = 0;
-    int64_t tile_faces_total = 0;
-    DevBuf<int2> cf;
-    DevBuf<double4> fgeo, cgeo;
-    DevBuf<double2> q[2];
-    DevBuf<double> w0, ecell, minit, ghost, partials, staging, wall_svec, wall_center, hist, scratch;
-    Control *ctl = nullptr;        // device
-    Control *ctl_host = nullptr;   // pinned mirror
-    int cur = 0;                   // q buffer holding the current state
-    int hist_cap = 0;
-
-    cudaGraphExec_t graph = nullptr;
-    int graph_iters = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t prof_ev[10] = {};
-
-    ~Solver() {
-        if (graph) cudaGraphExecDestroy(graph);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        for (auto e : prof_ev)
-            if (e) cudaEventDestroy(e);
-        DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell, &tile_halo_ptr, &tile_halo, &tile_face_ptr};
-        for (auto *b : ib) b->release();
-        tile_rec.release();
-        tile_rec_off.release();
-        q32[0].release();
-        q32[1].release();
-        cgeo32.release();
-        tile_rec32.release();
-        tile_rec32_off.release();
-        tile_contrib.release();
-        cf.release();
-        fgeo.release();
-        cgeo.release();
-        q[0].release();
-        q[1].release();
-        DevBuf<double> *db[] = {&w0, &ecell, &minit, &ghost, &partials, &staging, &wall_svec, &wall_center, &hist,
-                                &scratch};
-        for (auto *b : db) b->release();
-        if (ctl) cudaFree(ctl);
-        if (ctl_host) cudaFreeHost(ctl_host);
-        if (own_stream && stream) cudaStreamDestroy(stream);
-    }
-
-    int64_t state_size() const { return (int64_t)N + G; }
-
-    int64_t device_bytes() const {
-        return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
-                         tile_face_ptr.n) * 4 + (int64_t)cf.n * 8 + (int64_t)tile_rec.n * 40 + (int64_t)tile_rec_off.n * 8 +
-               (int64_t)tile_contrib.n * 2 + (int64_t)(q32[0].n + q32[1].n + cgeo32.n) * 16 + (int64_t)tile_rec32.n * 24 +
-               (int64_t)tile_rec32_off.n * 8 +
-               (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
-               (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
-                         hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
-    }
-
-    StageArgs stage_args(int in_buf, double alpha, int first, int last) {
-        StageArgs a{};
-        a.n_cells = N;
-        a.n_ghosts = G;
-        a.cptr = cptr.p;
-        a.cf = cf.p;
-        a.fgeo = fgeo.p;
-        a.cgeo = cgeo.p;
-        a.qin = q[in_buf].p;
-        a.qout = q[1 - in_buf].p;
-        a.w0 = w0.p;
-        a.ecell = ecell.p;
-        a.minit = minit.p;
-        a.ghost = ghost.p;
-        a.partials = partials.p;
-        a.ctl = ctl;
-        a.fs = fs;
-        a.gamma = prm.gamma;
-        a.cfl = prm.cfl;
-        a.alpha = alpha;
-        a.scheme = prm.scheme;
-        a.first_stage = first;
-        a.last_stage = last;
-        a.new2old = new2old_d.p;
-        a.tile_halo_ptr = tile_halo_ptr.p;
-        a.tile_halo = tile_halo.p;
-        a.tile_face_ptr = tile_face_ptr.p;
-        a.tile_rec = reinterpret_cast<const char *>(tile_rec.p);
-        a.tile_rec_off = tile_rec_off.p;
-        a.tile_contrib = tile_contrib.p;
-        a.max_contrib = max_contrib;
-        a.smem_cells = smem_cells;
-        a.smem_faces = smem_faces;
-        a.w0_stride = w0_stride;
-        a.fault = &ctl->fault;
-        a.prefetch_distance = prefetch_distance;
-        a.n_tiles = n_tiles;
-        a.pipe_grid = std::min(n_tiles, n_sm);
-        a.q32in = q32[in_buf].p;
-        a.q32out = q32[1 - in_buf].p;
-        a.tile_rec32 = reinterpret_cast<const char *>(tile_rec32.p);
-        a.tile_rec32_off = tile_rec32_off.p;
-        a.cgeo32 = cgeo32.p;
-        return a;
-    }
-
-    int variant = 0;                // stage-kernel variant picked by autotune()
-    float variant_ms[kStageVariants] = {};
-
-    void launch_stage(const StageArgs &a, int v = -1) {
-        if (v < 0) v = variant;
-        if (f32) launch_stage_f32(a, stream, v);
-        else if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
-        else launch_stage_fast(a, stream, v);
-    }
-
-    // Time every stage-kernel variant on this mesh and keep the fastest.  The trial launches
-    // read the current state and write only scratch: the other state buffer (overwritten by the
-    // next real stage anyway) and a copy of the ghost cells; W0, E and the RMS partials are
-    // untouched (not a last stage), so results do not depend on the tuning.
-    void autotune() {
-        DevBuf<double> ghost_copy;
-        ghost_copy.alloc(ghost.n);
-        E3D_CUDA(cudaMemcpyAsync(ghost_copy.p, ghost.p, ghost.n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-        StageArgs a = stage_args(cur, 0.0533, 1, 0);
-        a.ghost = ghost_copy.p;
-        const int reps = N > 200000 ? 3 : 10;
-        float best = 1e30f;
-        if (f32) {
-            prepare_tile_f32(tile32_smem);
-        } else if (tiles_ok) {
-            if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
-            else prepare_tile_fast(tile_smem, pipe_smem);
-        }
-        for (int v = 0; v < kStageVariants; v++) {
-            variant_ms[v] = -1.0f;
-            // FP32_FLUX mode has face-tile kernels only: variant 2 and 3 are its two register budgets
-            if (f32 ? v < 2 : ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok))) continue;
-            launch_stage(a, v);  // warm
-            E3D_CUDA(cudaEventRecord(ev0, stream));
-            for (int r = 0; r < reps; r++) launch_stage(a, v);
-            E3D_CUDA(cudaEventRecord(ev1, stream));
-            E3D_CUDA(cudaEventSynchronize(ev1));
-            float ms = 0.f;
-            E3D_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-            variant_ms[v] = ms / reps;
-            if (variant_ms[v] < best) {
-                best = variant_ms[v];
-                variant = v;
-            }
-        }
-        E3D_CUDA(cudaGetLastError());
-        ghost_copy.release();
-    }
-
-    CoeffArgs coeff_args(int buf, int run_mode, double *out) {
-        CoeffArgs c{};
-        c.n_wall = n_wall;
-        c.cell = wall_cell.p;
-        c.svec = wall_svec.p;
-        c.center = wall_center.p;
-        c.q = q[buf].p;
-        c.p_inf = fs.p;
-        c.cp_factor = cp_factor;
-        c.cref = prm.cref;
-        c.sref = prm.sref;
-        for (int k = 0; k < 3; k++) c.ref[k] = prm.ref_point[k];
-        c.axis[0] = prm.cl_axis;
-        c.axis[1] = prm.cd_axis;
-        c.axis[2] = prm.cm_axis;
-        c.sign[0] = prm.cl_sign;
-        c.sign[1] = prm.cd_sign;
-        c.sign[2] = prm.cm_sign;
-        c.ctl = ctl;
-        c.run_mode = run_mode;
-        c.sequential = prm.precision == E3D_PREC_FP64_EXACT;
-        c.w0 = f32 ? w0.p : nullptr;
-        c.w0_stride = w0_stride;
-        c.gamma = prm.gamma;
-        c.out = out;
-        return c;
-    }
-
-    // One RK5 iteration (EulerSolver.cpp:84-153) starting from q[in_buf]; returns launches.
-    int enqueue_iteration(int in_buf) {
-        static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
-        int b = in_buf;
-        for (int s = 0; s < 5; s++) {
-            launch_stage(stage_args(b, alphas[s], s == 0, s == 4));
-            b = 1 - b;
-        }
-        finalize_kernel<<<1, kReduceThreads, 0, stream>>>(partials.p, n_blocks, (double)N, hist.p, ctl);
-        coeff_kernel<<<1, kCoeffThreads, 0, stream>>>(coeff_args(b, 1, nullptr));
-        return 7;
-    }
-
-    void build_graph(int iters) {
-        if (graph && graph_iters == iters) return;
-        if (graph) {
-            cudaGraphExecDestroy(graph);
-            graph = nullptr;
-        }
-        cudaGraph_t g;
-        E3D_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        int b = 0;
-        for (int i = 0; i < iters; i++) {
-            enqueue_iteration(b);
-            b = 1 - b;  // five stages flip the buffer once per iteration
-        }
-        cudaError_t cap = cudaStreamEndCapture(stream, &g);
-        E3D_CUDA(cap);
-        cudaError_t inst = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        E3D_CUDA(inst);
-        graph_iters = iters;
-    }
-};
-
-static Solver *as_solver(e3d_solver *s) { return reinterpret_cast<Solver *>(s); }
 
 static void check_desc(const e3d_mesh_desc *d) {
     if (!d) throw Error(E3D_ERR_INVALID_ARG, "mesh descriptor is NULL");
@@ -1052,6 +815,80 @@ static void set_freestream(Solver *S) {
 
 using namespace e3d;
 
+namespace e3d {
+
+// A solver that is not a member of a batch (the batch owns its members' state and run).
+static Solver *solo(e3d_solver *s) {
+    Solver *S = as_solver(s);
+    if (S->batch) throw Error(E3D_ERR_INVALID_ARG, "solver is a member of a batch (retire or remove it first)");
+    return S;
+}
+
+// A fresh control block for a run -- a new EulerSolver's counters (_nbInteration = 0,
+// _CL = _CD = _CM = 0, src/solver/EulerSolver.cpp:21-58) -- keeping whether the loaded interior
+// Mach still holds.  Reads the old block back first (synchronises stream s once).
+static void init_control(Solver *S, const e3d_run_params *rp, int max_iter, int hist_cap, cudaStream_t s) {
+    E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
+    E3D_CUDA(cudaStreamSynchronize(s));
+    Control init{};
+    init.minit_valid = S->ctl_host->minit_valid;
+    init.max_iter = max_iter;
+    init.sampling = rp->sampling;
+    init.hist_cap = hist_cap;
+    init.min_res = rp->min_residual;
+    init.min_aero = rp->min_aerocoeff_error;
+    init.min_drop = rp->min_residual_drop;
+    init.done = max_iter == 0;
+    std::memcpy(S->ctl_host, &init, sizeof init);
+    E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, s));
+}
+
+// Runs start from state buffer 0 (their graphs and launch sequences assume it).
+static void state_to_buffer0(Solver *S, cudaStream_t s) {
+    if (S->cur == 0) return;
+    if (S->f32)
+        E3D_CUDA(cudaMemcpyAsync(S->q32[0].p, S->q32[1].p, 2 * (size_t)S->N * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                 s));
+    else
+        E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2), cudaMemcpyDeviceToDevice,
+                                 s));
+    S->cur = 0;
+}
+
+void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s) {
+    if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
+    if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
+    const int max_iter = std::max(rp->max_iter, 0);
+    if (S->hist_cap < max_iter || !S->hist.p) {
+        E3D_CUDA(cudaStreamSynchronize(s));
+        S->hist.release();
+        S->hist.alloc(std::max(max_iter, 1));
+        S->hist_cap = std::max(max_iter, 1);
+        if (S->graph) {  // the captured finalize kernels hold the old history pointer
+            cudaGraphExecDestroy(S->graph);
+            S->graph = nullptr;
+        }
+    }
+    init_control(S, rp, max_iter, S->hist_cap, s);
+    state_to_buffer0(S, s);
+}
+
+void stats_from_control(const Control &c, e3d_run_stats *st) {
+    st->iterations = c.it;
+    st->stop_reason = c.stop_reason;
+    st->n_rms = c.n_rms;
+    st->last_rms = c.last_rms;
+    st->cl = c.cl;
+    st->cd = c.cd;
+    st->cm = c.cm;
+    for (int k = 0; k < 3; k++) {
+        st->force[k] = c.force[k];
+        st->moment[k] = c.moment[k];
+    }
+}
+
+}  // namespace e3d
+
 extern "C" {
 
 e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *params, e3d_solver **out) {
@@ -1078,6 +915,7 @@ void e3d_solver_destroy(e3d_solver *solver) {
     if (!solver) return;
     Solver *S = as_solver(solver);
     cudaSetDevice(S->device);
+    batch_detach(S);
     if (S->stream) cudaStreamSynchronize(S->stream);
     delete S;
 }
@@ -1104,7 +942,7 @@ int64_t e3d_solver_state_size(const e3d_solver *solver) {
 e3d_status e3d_solver_set_state(e3d_solver *solver, const double *const state[8]) {
     return guarded([&] {
         if (!solver || !state) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         upload_state(S, state);
     });
@@ -1113,7 +951,7 @@ e3d_status e3d_solver_set_state(e3d_solver *solver, const double *const state[8]
 e3d_status e3d_solver_set_freestream(e3d_solver *solver) {
     return guarded([&] {
         if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         set_freestream(S);
     });
@@ -1122,7 +960,7 @@ e3d_status e3d_solver_set_freestream(e3d_solver *solver) {
 e3d_status e3d_solver_get_state(e3d_solver *solver, double *const state[8]) {
     return guarded([&] {
         if (!solver || !state) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         for (int k = 0; k < 8; k++)
             if (!state[k]) throw Error(E3D_ERR_INVALID_ARG, "state array is NULL");
         E3D_CUDA(cudaSetDevice(S->device));
@@ -1147,7 +985,7 @@ e3d_status e3d_solver_get_state(e3d_solver *solver, double *const state[8]) {
 e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt) {
     return guarded([&] {
         if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         const size_t N = (size_t)S->N;
         if (S->staging.n < 6 * N) throw Error(E3D_ERR_INVALID_ARG, "staging buffer too small");
@@ -1168,9 +1006,9 @@ e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt)
 e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double moment[3]) {
     return guarded([&] {
         if (!solver || !force || !moment) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
-        coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(S->cur, 0, S->scratch.p));
+        launch_coeff(S->coeff_args(S->cur, 0, S->scratch.p), S->stream);
         E3D_CUDA(cudaGetLastError());
         double h[6];
         E3D_CUDA(cudaMemcpyAsync(h, S->scratch.p, sizeof h, cudaMemcpyDeviceToHost, S->stream));
@@ -1185,44 +1023,12 @@ e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double m
 e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_stats *stats) {
     return guarded([&] {
         if (!solver || !rp) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
         e3d_run_stats st{};
         const int max_iter = std::max(rp->max_iter, 0);
-        // history buffer
-        if (S->hist_cap < max_iter || !S->hist.p) {
-            S->hist.release();
-            S->hist.alloc(std::max(max_iter, 1));
-            S->hist_cap = std::max(max_iter, 1);
-            if (S->graph) {  // the captured finalize kernels hold the old history pointer
-                cudaGraphExecDestroy(S->graph);
-                S->graph = nullptr;
-            }
-        }
-        // control block: a fresh EulerSolver's counters (_nbInteration = 0, _CL = _CD = _CM = 0)
-        Control init{};
-        init.minit_valid = S->ctl_host->minit_valid;
-        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
-        E3D_CUDA(cudaStreamSynchronize(S->stream));
-        init.minit_valid = S->ctl_host->minit_valid;
-        init.max_iter = max_iter;
-        init.sampling = rp->sampling;
-        init.hist_cap = S->hist_cap;
-        init.min_res = rp->min_residual;
-        init.min_aero = rp->min_aerocoeff_error;
-        init.done = max_iter == 0;
-        std::memcpy(S->ctl_host, &init, sizeof init);
-        E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
-        if (S->cur != 0) {
-            if (S->f32)
-                E3D_CUDA(cudaMemcpyAsync(S->q32[0].p, S->q32[1].p, 2 * (size_t)S->N * sizeof(float4),
-                                         cudaMemcpyDeviceToDevice, S->stream));
-            else
-                E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
-                                         cudaMemcpyDeviceToDevice, S->stream));
-            S->cur = 0;
-        }
+        begin_run(S, rp, S->stream);
         if (rp->stage_kernel > 0) {
             const int v = rp->stage_kernel - 1;
             if (v >= kStageVariants || (S->f32 ? v < 2 : ((v == 2 && !S->tiles_ok) || (v == 3 && !S->pipe_ok))))
@@ -1270,9 +1076,8 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
                     E3D_CUDA(cudaEventRecord(S->prof_ev[2 * st_i + 1], S->stream));
                     b = 1 - b;
                 }
-                finalize_kernel<<<1, kReduceThreads, 0, S->stream>>>(S->partials.p, S->n_blocks, (double)S->N,
-                                                                     S->hist.p, S->ctl);
-                coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
+                launch_finalize(S->finalize_args(S->partials.p, S->hist.p), S->stream);
+                launch_coeff(S->coeff_args(b, 1, nullptr), S->stream);
                 E3D_CUDA(cudaGetLastError());
                 launches += 7;
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
@@ -1293,17 +1098,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         E3D_CUDA(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
         const Control &c = *S->ctl_host;
         S->cur = c.n_rms & 1;
-        st.iterations = c.it;
-        st.stop_reason = c.stop_reason;
-        st.n_rms = c.n_rms;
-        st.last_rms = c.last_rms;
-        st.cl = c.cl;
-        st.cd = c.cd;
-        st.cm = c.cm;
-        for (int k = 0; k < 3; k++) {
-            st.force[k] = c.force[k];
-            st.moment[k] = c.moment[k];
-        }
+        stats_from_control(c, &st);
         st.device_ms = ms;
         st.kernel_launches = launches;
         st.stage_ms = stage_ms;
@@ -1351,7 +1146,7 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
                                   double *rms_history, int32_t history_capacity) {
     return guarded([&] {
         if (!solver || !rp) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
         const int max_iter = std::max(rp->max_iter, 0);
@@ -1366,27 +1161,9 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
         double *hist = partials + kNoAllocMaxBlocks;
         // the history region starts cleared, so no entry of an earlier call can be read back
         E3D_CUDA(cudaMemsetAsync(hist, 0, (size_t)std::max(max_iter, 1) * sizeof(double), S->stream));
-        Control init{};
-        E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
-        E3D_CUDA(cudaStreamSynchronize(S->stream));
-        init.minit_valid = S->ctl_host->minit_valid;
-        init.max_iter = max_iter;
-        init.sampling = rp->sampling;
-        init.hist_cap = kNoAllocMaxIter;
-        init.min_res = rp->min_residual;
-        init.min_aero = rp->min_aerocoeff_error;
-        init.done = max_iter == 0;
-        std::memcpy(S->ctl_host, &init, sizeof init);
-        E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, S->stream));
-        if (S->cur != 0) {
-            if (S->f32)
-                E3D_CUDA(cudaMemcpyAsync(S->q32[0].p, S->q32[1].p, 2 * (size_t)S->N * sizeof(float4),
-                                         cudaMemcpyDeviceToDevice, S->stream));
-            else
-                E3D_CUDA(cudaMemcpyAsync(S->q[0].p, S->q[1].p, 3 * (size_t)S->N * sizeof(double2),
-                                         cudaMemcpyDeviceToDevice, S->stream));
-            S->cur = 0;
-        }
+        if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
+        init_control(S, rp, max_iter, kNoAllocMaxIter, S->stream);
+        state_to_buffer0(S, S->stream);
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
         const int every = rp->check_every > 0 ? rp->check_every : 32;
         int64_t launches = 0;
@@ -1399,8 +1176,8 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
                 S->launch_stage(a);
                 b = 1 - b;
             }
-            finalize_kernel<<<1, kReduceThreads, 0, S->stream>>>(partials, S->n_blocks, (double)S->N, hist, S->ctl);
-            coeff_kernel<<<1, kCoeffThreads, 0, S->stream>>>(S->coeff_args(b, 1, nullptr));
+            launch_finalize(S->finalize_args(partials, hist), S->stream);
+            launch_coeff(S->coeff_args(b, 1, nullptr), S->stream);
             E3D_CUDA(cudaGetLastError());
             launches += 7;
             if ((it + 1) % every == 0 || it + 1 == max_iter) {
@@ -1417,17 +1194,7 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
         const Control &c = *S->ctl_host;
         S->cur = c.n_rms & 1;
         e3d_run_stats st{};
-        st.iterations = c.it;
-        st.stop_reason = c.stop_reason;
-        st.n_rms = c.n_rms;
-        st.last_rms = c.last_rms;
-        st.cl = c.cl;
-        st.cd = c.cd;
-        st.cm = c.cm;
-        for (int k = 0; k < 3; k++) {
-            st.force[k] = c.force[k];
-            st.moment[k] = c.moment[k];
-        }
+        stats_from_control(c, &st);
         st.device_ms = ms;
         st.kernel_launches = launches;
         if (stats) *stats = st;
@@ -1443,7 +1210,7 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
 e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count) {
     return guarded([&] {
         if (!solver || !count) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
-        Solver *S = as_solver(solver);
+        Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
         int n = std::min(S->ctl_host->n_rms, S->hist_cap);
         *count = n;

@@ -1,0 +1,344 @@
+// Host-side solver handle of the euler3d_b200 library, shared by the single-solver entry points
+// (solver.cu) and the batch of solvers (batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "common.hpp"
+#include "euler3d_b200.h"
+#include "stage.cuh"
+
+namespace e3d {
+
+void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant);
+void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
+void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
+void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
+void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
+void prepare_tile_f32(size_t smem_bytes);
+constexpr int kStageVariants = 4;  // gather (two register budgets), face tiles, pipelined face tiles
+
+constexpr int kReduceThreads = 256;
+constexpr int kCoeffThreads = 512;
+void prepare_batch_exact(size_t smem_bytes);
+void prepare_batch_fast(size_t smem_bytes);
+void prepare_batch_f32(size_t smem_bytes);
+void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+
+struct CoeffArgs {
+    int n_wall;
+    const int *__restrict__ cell;       // device cell of each wall face, reference wall order
+    const double *__restrict__ svec;    // 3 per wall face: full face normal
+    const double *__restrict__ center;  // 3 per wall face: face centre
+    const double2 *__restrict__ q;
+    const double *__restrict__ w0;      // FP32_FLUX mode: pressure from the double conservative state
+    int w0_stride;
+    double gamma;
+    double p_inf, cp_factor, cref, sref, ref[3];
+    int axis[3], sign[3];
+    Control *ctl;
+    int run_mode;                       // 1: sampled inside e3d_solver_run, apply the stop test
+    int sequential;                     // 1: sum in the reference's wall order (FP64_EXACT)
+    double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
+};
+
+// Arguments of the RMS / stop-test kernel of one solver.
+struct FinalizeArgs {
+    const double *partials;  // per-tile (per-block) sums of R_rho^2
+    int n_part;
+    double n_domain;         // interior cells
+    double *hist;            // RMS history
+    Control *ctl;
+};
+
+// Kernels of solver.cu, launched through these.
+void launch_finalize(const FinalizeArgs &f, cudaStream_t s);
+void launch_coeff(const CoeffArgs &c, cudaStream_t s);
+void launch_finalize_batch(const FinalizeArgs *f, const int *n_members, int grid, cudaStream_t s);
+void launch_coeff_batch(const CoeffArgs *c, const int *n_members, int parity, int grid, cudaStream_t s);
+void launch_control_gather(Control *const *ctl, const int *n_members, Control *out, int grid, cudaStream_t s);
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        if (count) E3D_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void upload(const std::vector<T> &v, cudaStream_t s) {
+        alloc(v.size());
+        if (n) E3D_CUDA(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+struct Batch;
+
+struct Solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int N = 0, G = 0, F = 0, Fint = 0;
+    e3d_flow_params prm{};
+    Freestream fs{};
+    double cp_factor = 0;
+    int n_wall = 0;
+    int n_blocks = 0;
+
+    std::vector<int> new2old, ghost_ref;  // host copies of the maps
+
+    DevBuf<int> cptr, new2old_d, ghost_ref_d, wall_cell, tile_halo_ptr, tile_halo, tile_face_ptr;
+    DevBuf<FaceRec> tile_rec;
+    DevBuf<long long> tile_rec_off;
+    bool f32 = false;                  // FP32_FLUX mode
+    DevBuf<float4> q32[2], cgeo32;
+    DevBuf<FaceRec32> tile_rec32;
+    DevBuf<long long> tile_rec32_off;
+    size_t tile32_smem = 0;
+    DevBuf<unsigned short> tile_contrib;
+    int w0_stride = 0;
+    int prefetch_distance = 0;  // tile_kernel L2 prefetch distance: resident blocks on the device
+    bool tiles_ok = false, pipe_ok = false;
+    size_t pipe_smem = 0;
+    int n_tiles = 0, n_sm = 0;
+    int max_contrib = 0, smem_cells = 0, smem_faces = 0;
+    size_t tile_smem = 0;
+    int64_t tile_faces_total = 0;
+    DevBuf<int2> cf;
+    DevBuf<double4> fgeo, cgeo;
+    DevBuf<double2> q[2];
+    DevBuf<double> w0, ecell, minit, ghost, partials, staging, wall_svec, wall_center, hist, scratch;
+    Control *ctl = nullptr;        // device
+    Control *ctl_host = nullptr;   // pinned mirror
+    int cur = 0;                   // q buffer holding the current state
+    int hist_cap = 0;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    Batch *batch = nullptr;        // the batch running this solver, if any (batch.cu)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t prof_ev[10] = {};
+
+    ~Solver() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto e : prof_ev)
+            if (e) cudaEventDestroy(e);
+        DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell, &tile_halo_ptr, &tile_halo, &tile_face_ptr};
+        for (auto *b : ib) b->release();
+        tile_rec.release();
+        tile_rec_off.release();
+        q32[0].release();
+        q32[1].release();
+        cgeo32.release();
+        tile_rec32.release();
+        tile_rec32_off.release();
+        tile_contrib.release();
+        cf.release();
+        fgeo.release();
+        cgeo.release();
+        q[0].release();
+        q[1].release();
+        DevBuf<double> *db[] = {&w0, &ecell, &minit, &ghost, &partials, &staging, &wall_svec, &wall_center, &hist,
+                                &scratch};
+        for (auto *b : db) b->release();
+        if (ctl) cudaFree(ctl);
+        if (ctl_host) cudaFreeHost(ctl_host);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    int64_t state_size() const { return (int64_t)N + G; }
+
+    int64_t device_bytes() const {
+        return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
+                         tile_face_ptr.n) * 4 + (int64_t)cf.n * 8 + (int64_t)tile_rec.n * 40 + (int64_t)tile_rec_off.n * 8 +
+               (int64_t)tile_contrib.n * 2 + (int64_t)(q32[0].n + q32[1].n + cgeo32.n) * 16 + (int64_t)tile_rec32.n * 24 +
+               (int64_t)tile_rec32_off.n * 8 +
+               (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
+               (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
+                         hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
+    }
+
+    StageArgs stage_args(int in_buf, double alpha, int first, int last) {
+        StageArgs a{};
+        a.n_cells = N;
+        a.n_ghosts = G;
+        a.cptr = cptr.p;
+        a.cf = cf.p;
+        a.fgeo = fgeo.p;
+        a.cgeo = cgeo.p;
+        a.qin = q[in_buf].p;
+        a.qout = q[1 - in_buf].p;
+        a.w0 = w0.p;
+        a.ecell = ecell.p;
+        a.minit = minit.p;
+        a.ghost = ghost.p;
+        a.partials = partials.p;
+        a.ctl = ctl;
+        a.fs = fs;
+        a.gamma = prm.gamma;
+        a.cfl = prm.cfl;
+        a.alpha = alpha;
+        a.scheme = prm.scheme;
+        a.first_stage = first;
+        a.last_stage = last;
+        a.new2old = new2old_d.p;
+        a.tile_halo_ptr = tile_halo_ptr.p;
+        a.tile_halo = tile_halo.p;
+        a.tile_face_ptr = tile_face_ptr.p;
+        a.tile_rec = reinterpret_cast<const char *>(tile_rec.p);
+        a.tile_rec_off = tile_rec_off.p;
+        a.tile_contrib = tile_contrib.p;
+        a.max_contrib = max_contrib;
+        a.smem_cells = smem_cells;
+        a.smem_faces = smem_faces;
+        a.w0_stride = w0_stride;
+        a.fault = &ctl->fault;
+        a.prefetch_distance = prefetch_distance;
+        a.n_tiles = n_tiles;
+        a.pipe_grid = std::min(n_tiles, n_sm);
+        a.q32in = q32[in_buf].p;
+        a.q32out = q32[1 - in_buf].p;
+        a.tile_rec32 = reinterpret_cast<const char *>(tile_rec32.p);
+        a.tile_rec32_off = tile_rec32_off.p;
+        a.cgeo32 = cgeo32.p;
+        return a;
+    }
+
+    int variant = 0;                // stage-kernel variant picked by autotune()
+    float variant_ms[kStageVariants] = {};
+
+    void launch_stage(const StageArgs &a, int v = -1) {
+        if (v < 0) v = variant;
+        if (f32) launch_stage_f32(a, stream, v);
+        else if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
+        else launch_stage_fast(a, stream, v);
+    }
+
+    // Time every stage-kernel variant on this mesh and keep the fastest.  The trial launches
+    // read the current state and write only scratch: the other state buffer (overwritten by the
+    // next real stage anyway) and a copy of the ghost cells; W0, E and the RMS partials are
+    // untouched (not a last stage), so results do not depend on the tuning.
+    void autotune() {
+        DevBuf<double> ghost_copy;
+        ghost_copy.alloc(ghost.n);
+        E3D_CUDA(cudaMemcpyAsync(ghost_copy.p, ghost.p, ghost.n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        StageArgs a = stage_args(cur, 0.0533, 1, 0);
+        a.ghost = ghost_copy.p;
+        const int reps = N > 200000 ? 3 : 10;
+        float best = 1e30f;
+        if (f32) {
+            prepare_tile_f32(tile32_smem);
+        } else if (tiles_ok) {
+            if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
+            else prepare_tile_fast(tile_smem, pipe_smem);
+        }
+        for (int v = 0; v < kStageVariants; v++) {
+            variant_ms[v] = -1.0f;
+            // FP32_FLUX mode has face-tile kernels only: variant 2 and 3 are its two register budgets
+            if (f32 ? v < 2 : ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok))) continue;
+            launch_stage(a, v);  // warm
+            E3D_CUDA(cudaEventRecord(ev0, stream));
+            for (int r = 0; r < reps; r++) launch_stage(a, v);
+            E3D_CUDA(cudaEventRecord(ev1, stream));
+            E3D_CUDA(cudaEventSynchronize(ev1));
+            float ms = 0.f;
+            E3D_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            variant_ms[v] = ms / reps;
+            if (variant_ms[v] < best) {
+                best = variant_ms[v];
+                variant = v;
+            }
+        }
+        E3D_CUDA(cudaGetLastError());
+        ghost_copy.release();
+    }
+
+    CoeffArgs coeff_args(int buf, int run_mode, double *out) {
+        CoeffArgs c{};
+        c.n_wall = n_wall;
+        c.cell = wall_cell.p;
+        c.svec = wall_svec.p;
+        c.center = wall_center.p;
+        c.q = q[buf].p;
+        c.p_inf = fs.p;
+        c.cp_factor = cp_factor;
+        c.cref = prm.cref;
+        c.sref = prm.sref;
+        for (int k = 0; k < 3; k++) c.ref[k] = prm.ref_point[k];
+        c.axis[0] = prm.cl_axis;
+        c.axis[1] = prm.cd_axis;
+        c.axis[2] = prm.cm_axis;
+        c.sign[0] = prm.cl_sign;
+        c.sign[1] = prm.cd_sign;
+        c.sign[2] = prm.cm_sign;
+        c.ctl = ctl;
+        c.run_mode = run_mode;
+        c.sequential = prm.precision == E3D_PREC_FP64_EXACT;
+        c.w0 = f32 ? w0.p : nullptr;
+        c.w0_stride = w0_stride;
+        c.gamma = prm.gamma;
+        c.out = out;
+        return c;
+    }
+
+    FinalizeArgs finalize_args(const double *part, double *h) const {
+        return FinalizeArgs{part, n_blocks, (double)N, h, ctl};
+    }
+
+    // One RK5 iteration (src/solver/EulerSolver.cpp:84-153) starting from q[in_buf]; returns launches.
+    int enqueue_iteration(int in_buf) {
+        static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+        int b = in_buf;
+        for (int s = 0; s < 5; s++) {
+            launch_stage(stage_args(b, alphas[s], s == 0, s == 4));
+            b = 1 - b;
+        }
+        launch_finalize(finalize_args(partials.p, hist.p), stream);
+        launch_coeff(coeff_args(b, 1, nullptr), stream);
+        return 7;
+    }
+
+    void build_graph(int iters) {
+        if (graph && graph_iters == iters) return;
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+        cudaGraph_t g;
+        E3D_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int b = 0;
+        for (int i = 0; i < iters; i++) {
+            enqueue_iteration(b);
+            b = 1 - b;  // five stages flip the buffer once per iteration
+        }
+        cudaError_t cap = cudaStreamEndCapture(stream, &g);
+        E3D_CUDA(cap);
+        cudaError_t inst = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        E3D_CUDA(inst);
+        graph_iters = iters;
+    }
+};
+
+inline Solver *as_solver(e3d_solver *s) { return reinterpret_cast<Solver *>(s); }
+
+// Start of a run (e3d_solver_run and e3d_batch_add): history capacity, a fresh control block
+// and the current state moved to buffer 0, all enqueued on stream s.
+void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s);
+// Run statistics from a control block read back from the device.
+void stats_from_control(const Control &c, e3d_run_stats *st);
+// Take a solver out of the batch that holds it (e3d_solver_destroy of a member).
+void batch_detach(Solver *S);
+
+}  // namespace e3d

@@ -45,6 +45,8 @@ struct Control {
     int max_iter, sampling, hist_cap;
     int fault;         // a bounded wait in a kernel gave up
     double min_res, min_aero, last_rms, cl, cd, cm;
+    double min_drop;   // > 0: also stop once the RMS is below min_drop x the run's first RMS
+    double rms0;       // RMS of the run's first iteration
     double force[3], moment[3];
 };
 
@@ -808,10 +810,10 @@ __device__ __forceinline__ bool tile_wait(const StageArgs &a, uint64_t *bar, uin
 
 // ---- one block per tile, all loads issued at the start (variant 2)
 // Shared memory: TileBuf | fs[5][FC] | sq[2][LC] | mbarrier
+// The body is shared by tile_kernel (one solver) and tile_batch_kernel (several solvers in one
+// grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
 template <bool EXACT>
-__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *partial, unsigned char *smem_raw) {
     const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
     const TileBuf b = tile_buf_at(smem_raw, LC, FC, MC);
     size_t off = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
@@ -819,7 +821,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
     double *sq = fs + 5 * FC;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
 
-    const int tile = blockIdx.x, c0 = tile * T;
+    const int c0 = tile * T;
     const int nloc = min(T, a.n_cells - c0);
     const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
     const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
@@ -842,7 +844,56 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
     __syncthreads();
     double r2 = 0.0;
     if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
-    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, partial);
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tile_body<EXACT>(a, blockIdx.x, a.partials + blockIdx.x, smem_raw);
+}
+
+// ---- several solvers ("members") in one grid
+// The face tiles of every member are concatenated into one launch: block k handles tile
+// table[k].y of member table[k].x with that member's own arguments (mesh, state buffers, flow
+// conditions, CFL, run control).  Members are independent, so each one computes exactly what its
+// own tile_kernel launch would: the same tiles, the same per-cell face order and the same RMS
+// partials.  A member whose run has stopped (its done flag) costs its blocks one load.
+struct BatchStage {
+    const StageArgs *__restrict__ args;  // member m reading state buffer b: args[2 * m + b]
+    const int2 *__restrict__ table;      // block -> (member, tile of that member)
+    const int *__restrict__ n_entries;   // valid table entries; later blocks return at once
+    double alpha;
+    int first_stage, last_stage, parity;
+};
+static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied in 8-byte words");
+
+// The block's member arguments into shared memory, with the stage's own alpha and flags.
+__device__ __forceinline__ int2 batch_stage_args(const BatchStage &bs, StageArgs *sa) {
+    const int2 e = bs.table[blockIdx.x];
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(bs.args + 2 * e.x + bs.parity);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(sa);
+    for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / 8); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sa->alpha = bs.alpha;
+        sa->first_stage = bs.first_stage;
+        sa->last_stage = bs.last_stage;
+        sa->residual_only = 0;
+    }
+    __syncthreads();
+    return e;
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads, 2) tile_batch_kernel(BatchStage bs) {
+    if ((int)blockIdx.x >= *bs.n_entries) return;  // uniform across the block
+    __shared__ __align__(16) StageArgs sa;
+    const int2 e = batch_stage_args(bs, &sa);
+    if (sa.ctl->done) return;  // uniform across the member's blocks
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tile_body<EXACT>(sa, e.y, sa.partials + e.y, smem_raw);
 }
 
 // ---- persistent, double-buffered (variant 3)

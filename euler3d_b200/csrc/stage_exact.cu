@@ -1,15 +1,21 @@
 // FP64_EXACT instantiations of the stage kernels.  Built with -fmad=false so that every double
 // operation rounds exactly as the reference's source order does.
+#include "common.hpp"
 #include "stage.cuh"
 
 namespace e3d {
 
-// Dynamic shared memory the tile kernels may use (set before their first launch).
+// Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes) {
-    cudaFuncSetAttribute(tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (pipe_smem_bytes)
-        cudaFuncSetAttribute(tile_pipe_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)pipe_smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<true>, smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<true>, pipe_smem_bytes);
+}
+
+void prepare_batch_exact(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<true>, smem_bytes); }
+
+// One stage of every member of a batch: `grid` blocks over the (member, tile) table.
+void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
+    tile_batch_kernel<true><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, 1 block(s)/SM register budget; 1: gather kernel, 2 blocks/SM;

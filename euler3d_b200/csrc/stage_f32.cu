@@ -1,11 +1,19 @@
 // FP32_FLUX instantiations of the face-tile stage kernel.
+#include "common.hpp"
 #include "stage_f32.cuh"
 
 namespace e3d {
 
 void prepare_tile_f32(size_t smem_bytes) {
-    cudaFuncSetAttribute(tile_kernel_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    cudaFuncSetAttribute(tile_kernel_f32<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    raise_smem_limit((const void *)tile_kernel_f32<2>, smem_bytes);
+    raise_smem_limit((const void *)tile_kernel_f32<3>, smem_bytes);
+}
+
+void prepare_batch_f32(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel_f32<3>, smem_bytes); }
+
+// One stage of every member of a batch: `grid` blocks over the (member, tile) table.
+void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
+    tile_batch_kernel_f32<3><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 2: two blocks/SM register budget; 3: three blocks/SM

@@ -121,10 +121,9 @@ inline size_t tile32_smem_bytes(int smem_cells, int smem_faces, int max_contrib)
     return b + 16;
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// Body shared by tile_kernel_f32 (one solver) and tile_batch_kernel_f32 (several solvers in one
+// grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
+__device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, double *partial, unsigned char *smem_raw) {
     const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
     size_t off = 0;
     float4 *st = reinterpret_cast<float4 *>(smem_raw + off);
@@ -142,7 +141,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs
     off += (size_t)5 * FC * 4;
     off = (off + 15) & ~(size_t)15;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
-    const int tile = blockIdx.x, c0 = tile * T;
+    const int c0 = tile * T;
     const int nloc = min(T, a.n_cells - c0);
     const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
     const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
@@ -251,7 +250,25 @@ __global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs
             }
         }
     }
-    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, partial);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tile_body_f32(a, blockIdx.x, a.partials + blockIdx.x, smem_raw);
+}
+
+// Several solvers in one grid (see tile_batch_kernel).
+template <int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB) tile_batch_kernel_f32(BatchStage bs) {
+    if ((int)blockIdx.x >= *bs.n_entries) return;
+    __shared__ __align__(16) StageArgs sa;
+    const int2 e = batch_stage_args(bs, &sa);
+    if (sa.ctl->done) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tile_body_f32(sa, e.y, sa.partials + e.y, smem_raw);
 }
 
 }  // namespace e3d

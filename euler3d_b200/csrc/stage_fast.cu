@@ -1,14 +1,20 @@
 // FP64 instantiations of the stage kernels: restructured arithmetic, FMA contraction allowed.
+#include "common.hpp"
 #include "stage.cuh"
 
 namespace e3d {
 
-// Dynamic shared memory the tile kernels may use (set before their first launch).
+// Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
-    cudaFuncSetAttribute(tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (pipe_smem_bytes)
-        cudaFuncSetAttribute(tile_pipe_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)pipe_smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<false>, smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<false>, pipe_smem_bytes);
+}
+
+void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false>, smem_bytes); }
+
+// One stage of every member of a batch: `grid` blocks over the (member, tile) table.
+void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
+    tile_batch_kernel<false><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;

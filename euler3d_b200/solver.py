@@ -164,6 +164,22 @@ class FlowConfig:
         return cl, cd, cm
 
 
+def run_params(max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
+               check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
+               min_residual_drop: float = 0.0) -> _lib.RunParams:
+    """``e3d_run_params``: MAX_ITER, SAMPLING, MIN_RESIDUAL, MIN_AEROCOEFF_ERROR of the reference's
+    config plus the launch options and the relative residual-drop stop."""
+    return _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages),
+                          stage_kernel, min_residual_drop)
+
+
+def stats_dict(st: _lib.RunStats) -> Dict[str, object]:
+    return {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,
+            "last_rms": st.last_rms, "cl": st.cl, "cd": st.cd, "cm": st.cm, "force": list(st.force),
+            "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches,
+            "stage_ms": st.stage_ms, "stage_launches": st.stage_launches}
+
+
 class EulerSolver:
     """GPU replacement of the reference's ``EulerSolver`` (include/solver/EulerSolver.hpp:89-223)."""
 
@@ -225,15 +241,13 @@ class EulerSolver:
 
     # ---- hot path
     def run(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
-            check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0) -> Dict[str, object]:
-        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages),
-                            stage_kernel)
+            check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
+            min_residual_drop: float = 0.0) -> Dict[str, object]:
+        rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, profile_stages,
+                        stage_kernel, min_residual_drop)
         st = _lib.RunStats()
         status = _lib.load().e3d_solver_run(self._h, C.byref(rp), C.byref(st))
-        stats = {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,
-                 "last_rms": st.last_rms, "cl": st.cl, "cd": st.cd, "cm": st.cm, "force": list(st.force),
-                 "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches,
-                 "stage_ms": st.stage_ms, "stage_launches": st.stage_launches}
+        stats = stats_dict(st)
         check(status)
         return stats
 
@@ -242,14 +256,13 @@ class EulerSolver:
         """``e3d_solver_run_noalloc``: the same iterations as :meth:`run` without any device allocation
         (scratch in a fixed 1 MiB device array; at most 65,536 iterations per call).  Returns
         (stats, density RMS of every iteration)."""
-        rp = _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, 0, 0)
+        rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, check_every)
         st = _lib.RunStats()
         hist = np.zeros(max(max_iter, 1))
         status = _lib.load().e3d_solver_run_noalloc(self._h, C.byref(rp), C.byref(st), _dp(hist), hist.size)
         check(status)
-        stats = {"iterations": st.iterations, "stop_reason": st.stop_reason, "n_rms": st.n_rms,
-                 "last_rms": st.last_rms, "cl": st.cl, "cd": st.cd, "cm": st.cm, "force": list(st.force),
-                 "moment": list(st.moment), "device_ms": st.device_ms, "kernel_launches": st.kernel_launches}
+        stats = stats_dict(st)
+        del stats["stage_ms"], stats["stage_launches"]
         return stats, hist[: st.n_rms].copy()
 
     def rms_history(self) -> np.ndarray:

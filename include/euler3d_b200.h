@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define E3D_ABI_VERSION 1
+#define E3D_ABI_VERSION 2
 
 typedef enum e3d_status {
 	E3D_OK = 0,
@@ -181,6 +181,9 @@ typedef struct e3d_run_params {
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
 	                                     register budgets; 3: face tiles; 4: persistent double-buffered
 	                                     face tiles (kept for later runs) */
+	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
+	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
+	                                     No counterpart in the reference, whose test is absolute. */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {
@@ -226,6 +229,62 @@ e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt)
 
 /* AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52) on the current state. */
 e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double moment[3]);
+
+/* ------------------------------------------------------------------------------------------
+ * Batches: many solvers advanced together.  No counterpart in the reference, whose solver runs one
+ * mesh per process.
+ *
+ * A batch runs the RK iterations of its members -- solver handles of any mesh sizes and flow
+ * conditions, on one device and of one precision -- in shared launches: each Runge-Kutta stage is
+ * ONE kernel over the concatenated face tiles of every running member (block -> member, tile),
+ * each member's RMS and stop test and its force coefficients one block each of two more kernels,
+ * and a step's iterations are one CUDA graph.  Every member keeps its own state, CFL, scheme, stop
+ * criteria and iteration counters on the device; a member that meets its stop condition stops
+ * updating at once, while the others go on.  Each member computes exactly what e3d_solver_run with
+ * params->stage_kernel = 3 (face tiles) computes for it alone: same states, RMS history, counters
+ * and coefficients.
+ *
+ * A solver belongs to the batch from e3d_batch_add until it is retired or removed; meanwhile the
+ * other e3d_solver_* calls on it fail with E3D_ERR_INVALID_ARG (e3d_solver_destroy removes it).
+ * One host thread drives a batch at a time. */
+typedef struct e3d_batch e3d_batch;
+
+/* An empty batch on `device`, running on `stream` (cudaStream_t, or NULL for a batch-owned stream). */
+e3d_status e3d_batch_create(int32_t device, void *stream, e3d_batch **out);
+/* Removes every member (their state stays on the device, usable again) and frees the batch. */
+void e3d_batch_destroy(e3d_batch *batch);
+
+/* Starts a run of `solver` inside the batch, as e3d_solver_run would start it: fresh counters, the
+ * solver's current state, params' stop criteria (params->stage_kernel, check_every and
+ * profile_stages are ignored).  The solver's mesh must fit the face-tile kernel. */
+e3d_status e3d_batch_add(e3d_batch *batch, e3d_solver *solver, const e3d_run_params *params);
+
+/* Runs `iterations` more iterations (rounded up to an even number) of every running member and
+ * waits for them.  n_active (may be NULL) receives how many members are still running. */
+e3d_status e3d_batch_step(e3d_batch *batch, int32_t iterations, int32_t *n_active);
+
+/* Takes up to `capacity` members whose runs have stopped out of the batch, in the order they were
+ * added: solvers[i] and (when not NULL) stats[i] -- the e3d_run_stats their e3d_solver_run would
+ * have returned, device_ms and kernel_launches being those of the batch steps they took part in --
+ * and status[i]: E3D_OK, E3D_ERR_NONFINITE or E3D_ERR_TIMEOUT as e3d_solver_run would return.
+ * *count receives the number taken. */
+e3d_status e3d_batch_retire(e3d_batch *batch, e3d_solver **solvers, e3d_run_stats *stats, e3d_status *status,
+                            int32_t capacity, int32_t *count);
+
+/* Takes `solver` out of the batch whether or not its run has stopped; stats as e3d_batch_retire. */
+e3d_status e3d_batch_remove(e3d_batch *batch, e3d_solver *solver, e3d_run_stats *stats);
+
+typedef struct e3d_batch_info {
+	int32_t n_members;                /* members (running or stopped, not yet retired) */
+	int32_t n_running;                /* members whose runs have not stopped */
+	int32_t n_tiles;                  /* face tiles in the stage launches of the last step */
+	int32_t graph_builds;             /* CUDA graphs instantiated so far */
+	int64_t member_device_bytes;      /* e3d_solver_info.device_bytes summed over the members */
+	int64_t device_bytes;             /* device memory held by the batch itself */
+	double last_step_ms;              /* device time of the last e3d_batch_step */
+	int64_t kernel_launches;          /* kernels launched by all steps so far */
+} e3d_batch_info;
+e3d_status e3d_batch_info_get(const e3d_batch *batch, e3d_batch_info *info);
 
 const char *e3d_status_string(e3d_status status);
 const char *e3d_last_error(void);

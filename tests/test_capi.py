@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_status_strings():
     lib = _lib.load()
-    assert lib.e3d_abi_version() == 1
+    assert lib.e3d_abi_version() == _lib.ABI_VERSION == 2
     assert lib.e3d_status_string(_lib.E3D_ERR_NONFINITE) == b"non-finite solution"
 
 
@@ -49,6 +49,25 @@ def test_null_arguments_are_rejected():
     assert b"NULL" in lib.e3d_last_error()
     assert lib.e3d_solver_run(None, None, None) == _lib.E3D_ERR_INVALID_ARG
     assert lib.e3d_mesh_read(None, 1.0, 0, C.byref(h)) == _lib.E3D_ERR_INVALID_ARG
+    n = C.c_int32()
+    assert lib.e3d_batch_create(0, None, None) == _lib.E3D_ERR_INVALID_ARG
+    assert lib.e3d_batch_add(None, None, None) == _lib.E3D_ERR_INVALID_ARG
+    assert lib.e3d_batch_step(None, 2, C.byref(n)) == _lib.E3D_ERR_INVALID_ARG
+    assert lib.e3d_batch_retire(None, None, None, None, 0, C.byref(n)) == _lib.E3D_ERR_INVALID_ARG
+    assert lib.e3d_batch_remove(None, None, None) == _lib.E3D_ERR_INVALID_ARG
+    assert lib.e3d_batch_info_get(None, None) == _lib.E3D_ERR_INVALID_ARG
+    lib.e3d_batch_destroy(None)
+
+
+def test_batch_refuses_without_gpu():
+    """No sm_100 device: creating a batch fails with a CUDA status instead of running elsewhere."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    assert _lib.load().e3d_batch_create(0, None, C.byref(h)) in (_lib.E3D_ERR_CUDA, _lib.E3D_ERR_INVALID_ARG)
+    assert not h.value
 
 
 def test_descriptor_validation():
