@@ -50,7 +50,31 @@ def parse():
     ap.add_argument("--kernel", type=int, default=0, help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined face tiles")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", choices=["all", "stage", "served"], default="all",
+                    help="stage: the RK-stage line only; served: the served-stream comparison only")
+    ap.add_argument("--served-requests", type=int, default=48)
+    ap.add_argument("--served-rate", type=float, default=20.0, help="Poisson arrivals per second (0: burst)")
+    ap.add_argument("--served-cells", type=int, nargs=2, default=(5_000, 50_000))
+    ap.add_argument("--served-max-iter", type=int, default=20_000)
     return ap.parse_args()
+
+
+def served_leg(args) -> dict:
+    """The served-stream comparison: a seeded Poisson stream of solve requests (bump-channel and
+    biconvex O-grid meshes, log-uniform cell counts, Mach 0.3-0.85, AoA -4..6 deg, Roe or AUSM,
+    residual-drop tolerance 1e-6 or 1e-8, at most ``served_max_iter`` iterations each) served with
+    continuous batching in FP64, then the same stream solved one at a time (plain FP64 path)."""
+    from euler3d_b200 import _lib, serve
+
+    lo, hi = args.served_cells
+    reqs = serve.request_stream(args.served_requests, args.served_rate, cells=(lo, hi), seed=4,
+                                drops=(1e-6, 1e-8), schemes=(_lib.SCHEME_ROE, _lib.SCHEME_AUSM))
+    out = serve.compare(reqs, _lib.PREC_FP64, max_iter=args.served_max_iter)
+    out["workload"] = (f"{args.served_requests} requests, Poisson {args.served_rate:g}/s (seed 4), "
+                       f"cells log-uniform [{lo}, {hi}], Mach 0.3-0.85, AoA -4..6, Roe/AUSM, drop 1e-6/1e-8, "
+                       f"max_iter {args.served_max_iter}")
+    out["metric"] = "served solves/s, p50/p99 latency"
+    return out
 
 
 def algorithmic_bytes_per_cell_stage(n_cells: int, n_faces: int, fp32: bool = False) -> float:
@@ -155,6 +179,11 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.mode == "served":
+        if rank == 0:
+            print(json.dumps({"metric": "served solves/s", "n_gpus": 1, "served": served_leg(args)}), flush=True)
+        return
 
     t0 = time.time()
     raw = meshgen.bump_box_tets(args.n)
@@ -265,9 +294,12 @@ def run_ours(args, rank, world, local_rank):
                      "avg_launch_ms": stage_ms, "autotune": solver.info()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
     }
+    solver.close()
+    del arrays
+    if rank == 0 and world == 1 and args.mode == "all" and args.served_requests > 0:
+        line["served"] = served_leg(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -43,7 +43,8 @@ class FlowParams(C.Structure):
                 ("sref", C.c_double), ("cref", C.c_double), ("ref_point", C.c_double * 3),
                 ("cl_axis", C.c_int32), ("cl_sign", C.c_int32), ("cd_axis", C.c_int32), ("cd_sign", C.c_int32),
                 ("cm_axis", C.c_int32), ("cm_sign", C.c_int32), ("scheme", C.c_int32), ("precision", C.c_int32),
-                ("ordering", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p)]
+                ("ordering", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
+                ("no_autotune", C.c_int32)]
 
 
 class RunParams(C.Structure):

@@ -905,7 +905,8 @@ e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *p
     e3d_status st = guarded([&] {
         create_solver(mesh, params, S.get());
         set_freestream(S.get());
-        S->autotune();
+        if (params->no_autotune) S->use_default_variant();
+        else S->autotune();
     });
     if (st == E3D_OK) *out = reinterpret_cast<e3d_solver *>(S.release());
     return st;

@@ -661,7 +661,8 @@ __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15
 //   rec[FC]  FaceRec of every face touching the tile (one bulk copy)
 //   w0[5][T], cg[T], ct[MC][T]   W0, cell geometry and contribution lists (bulk copies)
 // Evaluation: every face touching the tile is evaluated once (a face shared with another tile is
-// evaluated by both) and F*S kept in fs[5][FC]; each cell then sums its faces' F*S in ascending
+// evaluated by both) and its F*S (5 doubles, 40 bytes) written over the face's own 40-byte record,
+// which only the thread evaluating the face reads; each cell then sums its faces' F*S in ascending
 // reference face id, the order of the reference's face loop, so results are deterministic and, in
 // exact mode, the reference's bit for bit.
 struct TileBuf {
@@ -729,7 +730,7 @@ __device__ __forceinline__ void tile_roots(const StageArgs &a, const TileBuf &b,
     }
 }
 
-// One flux per tile face, F*S into fs.
+// One flux per tile face; F*S of face j replaces record j (fs[5 j + k] aliases b.rec[j]).
 template <bool EXACT, int NT>
 __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, const double *sq, double *fs,
                                             int LC, int FC, int nf, int c0) {
@@ -764,8 +765,10 @@ __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b
                 }
             }
         }
+        // the record is in registers; keep the compiler from moving its loads past the overwrite
+        asm volatile("" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 5; k++) fs[k * FC + j] = F[k] * fg.w;
+        for (int k = 0; k < 5; k++) fs[5 * j + k] = F[k] * fg.w;
     }
 }
 
@@ -790,10 +793,10 @@ __device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf 
         const int j = e[k] >> 1;
         if (e[k] & 1) {
 #pragma unroll
-            for (int q = 0; q < 5; q++) R[q] -= fs[q * FC + j];
+            for (int q = 0; q < 5; q++) R[q] -= fs[5 * j + q];
         } else {
 #pragma unroll
-            for (int q = 0; q < 5; q++) R[q] += fs[q * FC + j];
+            for (int q = 0; q < 5; q++) R[q] += fs[5 * j + q];
         }
     }
     return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : sq[LC + i], R, W0, cg);
@@ -809,7 +812,7 @@ __device__ __forceinline__ bool tile_wait(const StageArgs &a, uint64_t *bar, uin
 }
 
 // ---- one block per tile, all loads issued at the start (variant 2)
-// Shared memory: TileBuf | fs[5][FC] | sq[2][LC] | mbarrier
+// Shared memory: TileBuf (face fluxes over the records) | sq[2][LC] | mbarrier
 // The body is shared by tile_kernel (one solver) and tile_batch_kernel (several solvers in one
 // grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
 template <bool EXACT>
@@ -817,8 +820,8 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *
     const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
     const TileBuf b = tile_buf_at(smem_raw, LC, FC, MC);
     size_t off = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
-    double *fs = reinterpret_cast<double *>(smem_raw + off);
-    double *sq = fs + 5 * FC;
+    double *fs = reinterpret_cast<double *>(b.rec);
+    double *sq = reinterpret_cast<double *>(smem_raw + off);
     uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
 
     const int c0 = tile * T;
@@ -900,7 +903,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) tile_batch_kernel(BatchStage
 // One block of kPipeThreads per SM walks tiles blockIdx.x, +gridDim.x, ...  While it evaluates
 // tile i from one buffer, the bulk copies and halo gathers of tile i+1 fill the other, so memory
 // traffic overlaps computation.  Halo indices are read into registers one tile ahead of their use.
-// Shared memory: TileBuf x 2 | fs[5][FC] | sq[2][LC] | mbarrier x 2
+// Shared memory: TileBuf x 2 (face fluxes over each buffer's records) | sq[2][LC] | mbarrier x 2
 constexpr int kPipeThreads = 512;
 
 template <bool EXACT>
@@ -920,8 +923,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         r.ct = k ? buf1.ct : buf0.ct;
         return r;
     };
-    double *fs = reinterpret_cast<double *>(smem_raw + 2 * bb);
-    double *sq = fs + 5 * FC;
+    double *sq = reinterpret_cast<double *>(smem_raw + 2 * bb);
     uint64_t *bars = reinterpret_cast<uint64_t *>(sq + 2 * LC);
     const int G = gridDim.x;
     int tile = blockIdx.x;
@@ -979,12 +981,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
             tile_roots<kPipeThreads>(a, b, sq, LC, nloc + nh);
             __syncthreads();
         }
+        double *fs = reinterpret_cast<double *>(b.rec);
         tile_fluxes<EXACT, kPipeThreads>(a, b, sq, fs, LC, FC, nf, c0);
         __syncthreads();
         double r2 = 0.0;
         if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
         if (a.last_stage && !a.residual_only) block_sum_store<kPipeThreads>(r2, a.partials + tile);
-        __syncthreads();  // buffer cur, fs and sq are free again
+        __syncthreads();  // buffer cur (with its fluxes) and sq are free again
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
@@ -994,7 +997,7 @@ inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib, i
     size_t bb = (size_t)smem_cells * 48 + ((40u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
                 kTileCells * 32 + (size_t)max_contrib * kTileCells * 2;
     bb = (bb + 15) & ~(size_t)15;
-    size_t b = buffers * bb + 5 * (size_t)smem_faces * 8 + 2 * (size_t)smem_cells * 8;
+    size_t b = buffers * bb + 2 * (size_t)smem_cells * 8;
     b = (b + 15) & ~(size_t)15;
     return b + 16;
 }

@@ -110,13 +110,13 @@ __device__ __forceinline__ PrimF prim32(const float4 *st, int i) {
     return PrimF{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 }
 
-// Shared memory: st[LC] 32-byte records | rec[FC] | w0[5][T] (double) | cg[T] | ct[MC][T] | fs[5][FC] (float)
+// Shared memory: st[LC] 32-byte records | rec[FC] | w0[5][T] (double) | cg[T] | ct[MC][T] | mbarrier.
+// The five float F*S of face j are written over its 24-byte record (fs[6 j + k]), which only the
+// thread evaluating the face reads.
 // | mbarrier
 inline size_t tile32_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
     size_t b = (size_t)smem_cells * 32 + ((24u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
                kTileCells * 16 + (size_t)max_contrib * kTileCells * 2;
-    b = (b + 15) & ~(size_t)15;
-    b += 5 * (size_t)smem_faces * 4;
     b = (b + 15) & ~(size_t)15;
     return b + 16;
 }
@@ -137,8 +137,7 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
     unsigned short *cts = reinterpret_cast<unsigned short *>(smem_raw + off);
     off += (size_t)MC * T * 2;
     off = (off + 15) & ~(size_t)15;
-    float *fs = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)5 * FC * 4;
+    float *fs = reinterpret_cast<float *>(rec);
     off = (off + 15) & ~(size_t)15;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
     const int c0 = tile * T;
@@ -199,8 +198,10 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
                 for (int k = 0; k < 5; k++) F[k] = (float)Fd[k];
             }
         }
+        // the record is in registers; keep the compiler from moving its loads past the overwrite
+        asm volatile("" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 5; k++) fs[k * FC + j] = F[k] * fr.S;
+        for (int k = 0; k < 5; k++) fs[6 * j + k] = F[k] * fr.S;
     }
     __syncthreads();
 
@@ -218,7 +219,7 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
             const int j = e[k] >> 1;
             const double sg = (e[k] & 1) ? -1.0 : 1.0;
 #pragma unroll
-            for (int q = 0; q < 5; q++) R[q] += sg * (double)fs[q * FC + j];
+            for (int q = 0; q < 5; q++) R[q] += sg * (double)fs[6 * j + q];
         }
         // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
         const float4 cg = cgs[i];

@@ -183,7 +183,7 @@ def stats_dict(st: _lib.RunStats) -> Dict[str, object]:
 class EulerSolver:
     """GPU replacement of the reference's ``EulerSolver`` (include/solver/EulerSolver.hpp:89-223)."""
 
-    def __init__(self, mesh, flow: FlowConfig, stream: Optional[int] = None):
+    def __init__(self, mesh, flow: FlowConfig, stream: Optional[int] = None, autotune: bool = True):
         lib = _lib.load()
         arrays = mesh.arrays() if isinstance(mesh, Mesh) else mesh
         self._desc = _Desc(arrays)
@@ -198,6 +198,7 @@ class EulerSolver:
         p.cm_axis, p.cm_sign = flow.cm
         p.scheme, p.precision, p.ordering, p.device = flow.scheme, flow.precision, flow.ordering, flow.device
         p.stream = stream
+        p.no_autotune = 0 if autotune else 1
         h = C.c_void_p()
         check(lib.e3d_solver_create(C.byref(self._desc.c), C.byref(p), C.byref(h)))
         self._h = h

@@ -138,6 +138,8 @@ typedef struct e3d_flow_params {
 	int32_t ordering;                 /* E3D_ORDER_* */
 	int32_t device;                   /* CUDA device ordinal */
 	void *stream;                     /* cudaStream_t to run on, or NULL for a library-owned stream */
+	int32_t no_autotune;              /* 1: skip the creation-time timing of the stage-kernel variants
+	                                     and use the face-tile kernel (what a batch runs anyway) */
 } e3d_flow_params;
 
 typedef struct e3d_solver e3d_solver;
