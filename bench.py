@@ -289,7 +289,7 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
                      "kernel": (["-", "-", "tile_kernel_f32<2>", "tile_kernel_f32<3>"] if args.precision == "fp32" else
                                 ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>",
-                                 "tile_pipe_kernel<false>"])[solver.info()["stage_variant"]],
+                                 "tile_pipe_kernel<false>", "tile_kernel<false,3>"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "autotune": solver.info()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,

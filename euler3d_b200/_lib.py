@@ -16,7 +16,7 @@ E3D_OK, E3D_ERR_INVALID_ARG, E3D_ERR_OOM, E3D_ERR_NONFINITE, E3D_ERR_TIMEOUT, E3
 SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
 ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE = 0, 1, 2, 3, 4
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE, KERNEL_TILE_B3 = 0, 1, 2, 3, 4, 5
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
@@ -62,8 +62,8 @@ class RunStats(C.Structure):
 
 class SolverInfo(C.Structure):
     _fields_ = [("n_cells", C.c_int32), ("n_ghosts", C.c_int32), ("n_faces", C.c_int32),
-                ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 4),
-                ("device_bytes", C.c_int64)]
+                ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 5),
+                ("tile_smem_bytes", C.c_int32), ("device_bytes", C.c_int64)]
 
 
 class BatchInfo(C.Structure):

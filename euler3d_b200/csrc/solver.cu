@@ -931,7 +931,8 @@ e3d_status e3d_solver_info_get(const e3d_solver *solver, e3d_solver_info *info) 
         info->n_faces = S->F;
         info->stage_variant = S->variant;
         info->n_variants = kStageVariants;
-        for (int v = 0; v < kStageVariants && v < 4; v++) info->variant_ms[v] = S->variant_ms[v];
+        for (int v = 0; v < kStageVariants; v++) info->variant_ms[v] = S->variant_ms[v];
+        info->tile_smem_bytes = (int32_t)(S->f32 ? S->tile32_smem : S->tile_smem);
         info->device_bytes = S->device_bytes();
     });
 }
@@ -1032,7 +1033,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         begin_run(S, rp, S->stream);
         if (rp->stage_kernel > 0) {
             const int v = rp->stage_kernel - 1;
-            if (v >= kStageVariants || (S->f32 ? v < 2 : ((v == 2 && !S->tiles_ok) || (v == 3 && !S->pipe_ok))))
+            if (!S->variant_ok(v))
                 throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh and precision");
             if (S->f32) prepare_tile_f32(S->tile32_smem);
             else if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);

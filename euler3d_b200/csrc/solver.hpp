@@ -19,7 +19,8 @@ void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
 void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_f32(size_t smem_bytes);
-constexpr int kStageVariants = 4;  // gather (two register budgets), face tiles, pipelined face tiles
+// gather (two register budgets), face tiles, pipelined face tiles, face tiles at 3 blocks/SM
+constexpr int kStageVariants = 5;
 
 constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
@@ -218,6 +219,18 @@ struct Solver {
     int variant = 0;                // stage-kernel variant picked by autotune()
     float variant_ms[kStageVariants] = {};
 
+    // Variants compiled for this precision and possible on this mesh.  FP32_FLUX mode has face-tile
+    // kernels only (variants 2 and 3 are its two register budgets); the three-blocks-per-SM face-tile
+    // kernel exists for FP64 only (in FP64_EXACT it would spill).
+    bool variant_ok(int v) const {
+        if (v < 0 || v >= kStageVariants) return false;
+        if (f32) return v == 2 || v == 3;
+        if (v == 2) return tiles_ok;
+        if (v == 3) return pipe_ok;
+        if (v == 4) return tiles_ok && prm.precision == E3D_PREC_FP64;
+        return true;
+    }
+
     void launch_stage(const StageArgs &a, int v = -1) {
         if (v < 0) v = variant;
         if (f32) launch_stage_f32(a, stream, v);
@@ -245,8 +258,7 @@ struct Solver {
         }
         for (int v = 0; v < kStageVariants; v++) {
             variant_ms[v] = -1.0f;
-            // FP32_FLUX mode has face-tile kernels only: variant 2 and 3 are its two register budgets
-            if (f32 ? v < 2 : ((v == 2 && !tiles_ok) || (v == 3 && !pipe_ok))) continue;
+            if (!variant_ok(v)) continue;
             launch_stage(a, v);  // warm
             E3D_CUDA(cudaEventRecord(ev0, stream));
             for (int r = 0; r < reps; r++) launch_stage(a, v);

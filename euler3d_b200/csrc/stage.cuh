@@ -659,7 +659,9 @@ __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15
 //   st[LC]   48-byte states: owned cells (one bulk copy) then halo cells (outside neighbours,
 //            gathered with cp.async)
 //   rec[FC]  FaceRec of every face touching the tile (one bulk copy)
-//   w0[5][T], cg[T], ct[MC][T]   W0, cell geometry and contribution lists (bulk copies)
+//   cg[T], ct[MC][T]   cell geometry and contribution lists (bulk copies)
+// W0 (only ever read by the thread that owns the cell) stays in global memory: its rows are
+// prefetched into L2 when the tile starts and read, coalesced, by the update.
 // Evaluation: every face touching the tile is evaluated once (a face shared with another tile is
 // evaluated by both) and its F*S (5 doubles, 40 bytes) written over the face's own 40-byte record,
 // which only the thread evaluating the face reads; each cell then sums its faces' F*S in ascending
@@ -668,22 +670,19 @@ __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15
 struct TileBuf {
     double2 *st;
     FaceRec *rec;
-    double *w0;
     double4 *cg;
     unsigned short *ct;
 };
 
-__device__ __forceinline__ size_t tile_buf_bytes(int LC, int FC, int MC) {
-    return (size_t)LC * 48 + ((40u * (size_t)FC + 15) & ~(size_t)15) + 5 * kTileCells * 8 + kTileCells * 32 +
-           (size_t)MC * kTileCells * 2;
+__host__ __device__ __forceinline__ size_t tile_buf_bytes(int LC, int FC, int MC) {
+    return (size_t)LC * 48 + ((40u * (size_t)FC + 15) & ~(size_t)15) + kTileCells * 32 + (size_t)MC * kTileCells * 2;
 }
 
 __device__ __forceinline__ TileBuf tile_buf_at(unsigned char *base, int LC, int FC, int MC) {
     TileBuf b;
     b.st = reinterpret_cast<double2 *>(base);
     b.rec = reinterpret_cast<FaceRec *>(base + (size_t)LC * 48);
-    b.w0 = reinterpret_cast<double *>(base + (size_t)LC * 48 + round16(40u * FC));
-    b.cg = reinterpret_cast<double4 *>(b.w0 + 5 * kTileCells);
+    b.cg = reinterpret_cast<double4 *>(base + (size_t)LC * 48 + round16(40u * FC));
     b.ct = reinterpret_cast<unsigned short *>(b.cg + kTileCells);
     return b;
 }
@@ -695,13 +694,13 @@ __device__ __forceinline__ void tile_issue_bulk(const StageArgs &a, int tile, co
     const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
     const uint32_t b_state = (uint32_t)nloc * 48u;
     const uint32_t b_rec = round16(40u * (uint32_t)nf);
-    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // reads past the tile stay inside the padded rows
+    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // stays inside the padded rows
     const uint32_t b_cg = (uint32_t)nloc * 32u;
     const uint32_t b_ct = (uint32_t)MC * T * 2u;
-    mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
+    mbar_expect_tx(bar, b_state + b_rec + b_cg + b_ct);
     bulk_g2s(b.st, a.qin + 3 * (size_t)c0, b_state, bar);
     bulk_g2s(b.rec, a.tile_rec + a.tile_rec_off[tile], b_rec, bar);
-    for (int k = 0; k < 5; k++) bulk_g2s(b.w0 + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
+    for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
     bulk_g2s(b.cg, a.cgeo + c0, b_cg, bar);
     bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
 }
@@ -784,7 +783,7 @@ __device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf 
     for (int k = 0; k < 6; k++) e[k] = k < a.max_contrib ? b.ct[k * T + i] : kNoContrib;
     double W0[5];
 #pragma unroll
-    for (int k = 0; k < 5; k++) W0[k] = b.w0[k * T + i];
+    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
     const double4 cg = b.cg[i];
     const Prim me = tile_prim(b.st, i);
 #pragma unroll
@@ -850,8 +849,8 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *
     if (a.last_stage && !a.residual_only) block_sum_store(r2, partial);
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(kStageThreads, 2) tile_kernel(StageArgs a) {
+template <bool EXACT, int MINB = 2>
+__global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel(StageArgs a) {
     if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     tile_body<EXACT>(a, blockIdx.x, a.partials + blockIdx.x, smem_raw);
@@ -918,7 +917,6 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         TileBuf r;
         r.st = k ? buf1.st : buf0.st;
         r.rec = k ? buf1.rec : buf0.rec;
-        r.w0 = k ? buf1.w0 : buf0.w0;
         r.cg = k ? buf1.cg : buf0.cg;
         r.ct = k ? buf1.ct : buf0.ct;
         return r;
@@ -994,9 +992,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
 
 // Dynamic shared memory of tile_kernel (buffers = 1) and tile_pipe_kernel (buffers = 2).
 inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib, int buffers = 1) {
-    size_t bb = (size_t)smem_cells * 48 + ((40u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
-                kTileCells * 32 + (size_t)max_contrib * kTileCells * 2;
-    bb = (bb + 15) & ~(size_t)15;
+    const size_t bb = (tile_buf_bytes(smem_cells, smem_faces, max_contrib) + 15) & ~(size_t)15;
     size_t b = buffers * bb + 2 * (size_t)smem_cells * 8;
     b = (b + 15) & ~(size_t)15;
     return b + 16;

@@ -7,6 +7,7 @@ namespace e3d {
 // Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     raise_smem_limit((const void *)tile_kernel<false>, smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<false, 3>, smem_bytes);
     if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<false>, pipe_smem_bytes);
 }
 
@@ -18,10 +19,14 @@ void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaSt
 }
 
 // variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;
-// 2: face tiles, one block per tile; 3: face tiles, persistent and double-buffered
+// 2: face tiles, one block per tile; 3: face tiles, persistent and double-buffered; 4: face tiles
+// with a three-blocks-per-SM register budget
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
-    if (variant == 3) {
+    if (variant == 4) {
+        const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
+        tile_kernel<false, 3><<<blocks, kStageThreads, smem, s>>>(a);
+    } else if (variant == 3) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, 2);
         tile_pipe_kernel<false><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
     } else if (variant == 2) {

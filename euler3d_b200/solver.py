@@ -220,6 +220,7 @@ class EulerSolver:
         check(_lib.load().e3d_solver_info_get(self._h, C.byref(i)))
         return {"n_cells": i.n_cells, "n_ghosts": i.n_ghosts, "n_faces": i.n_faces,
                 "stage_variant": i.stage_variant, "variant_ms": list(i.variant_ms)[: i.n_variants],
+                "tile_smem_bytes": i.tile_smem_bytes,
                 "device_bytes": i.device_bytes}
 
     # ---- state

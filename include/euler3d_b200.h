@@ -157,7 +157,9 @@ typedef struct e3d_solver_info {
 	int32_t n_cells, n_ghosts, n_faces;
 	int32_t stage_variant;            /* variant in use */
 	int32_t n_variants;
-	float variant_ms[4];              /* measured duration of one stage launch per variant */
+	float variant_ms[5];              /* measured duration of one stage launch per variant (-1: not
+	                                     available for this mesh and precision) */
+	int32_t tile_smem_bytes;          /* dynamic shared memory of one face-tile block (0: no tiles) */
 	int64_t device_bytes;             /* device memory held by the handle */
 } e3d_solver_info;
 e3d_status e3d_solver_info_get(const e3d_solver *solver, e3d_solver_info *info);
@@ -182,7 +184,8 @@ typedef struct e3d_run_params {
 	                                     events (stats.stage_ms); 0: CUDA graphs */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
 	                                     register budgets; 3: face tiles; 4: persistent double-buffered
-	                                     face tiles (kept for later runs) */
+	                                     face tiles; 5: face tiles at three blocks per SM (FP64 only)
+	                                     (kept for later runs) */
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
 	                                     No counterpart in the reference, whose test is absolute. */

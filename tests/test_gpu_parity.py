@@ -43,6 +43,7 @@ def assert_state_equal(gpu, ora, n_cells, ghost_E_rtol=0.0):
 
 
 KERNELS = [_lib.KERNEL_GATHER, _lib.KERNEL_GATHER_B, _lib.KERNEL_TILE, _lib.KERNEL_TILE_PIPE]
+FAST_KERNELS = KERNELS + [_lib.KERNEL_TILE_B3]  # FP64 only: face tiles at three blocks per SM
 ORDERINGS = [_lib.ORDER_NATIVE, _lib.ORDER_RCM, _lib.ORDER_SPATIAL]
 
 
@@ -195,7 +196,7 @@ def test_nonfinite_reported():
     assert s.run(2)["iterations"] == 2
 
 
-@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("kernel", FAST_KERNELS)
 def test_determinism(kernel):
     name = "ogrid"
     flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
@@ -211,16 +212,18 @@ def test_determinism(kernel):
 
 
 def test_fast_kernels_agree():
-    """The three FP64 stage kernels give the same state to round-off (different FMA grouping
-    and, for the tiles, per-face instead of per-cell sqrt reuse)."""
+    """The FP64 stage kernels give the same state to round-off (different FMA grouping and, for
+    the tiles, per-face instead of per-cell sqrt reuse); the two tile register budgets agree exactly."""
     name = "tets"
     flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
     arrays = prepared(name)
     states = []
-    for kernel in KERNELS:
+    for kernel in FAST_KERNELS:
         s = EulerSolver(arrays, flow)
         s.run(30, stage_kernel=kernel)
         states.append(s.get_state())
+    for k in STATE_KEYS:
+        assert np.array_equal(states[2][k], states[4][k]), k
     for k in ("rho", "p", "H"):
         for other in states[1:]:
             assert np.max(np.abs(other[k] - states[0][k]) / np.abs(states[0][k])) < 1e-12
@@ -230,9 +233,12 @@ def test_autotune_info():
     name = "tets"
     s = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL))
     info = s.info()
-    assert len(info["variant_ms"]) == 4 and 0 <= info["stage_variant"] < 4
-    assert all(t > 0 for t in info["variant_ms"])
+    assert len(info["variant_ms"]) == 5 and 0 <= info["stage_variant"] < 5
+    assert all(t > 0 for t in info["variant_ms"])  # FP64: every variant runs on this mesh
     assert info["variant_ms"][info["stage_variant"]] == min(info["variant_ms"])
+    assert 0 < info["tile_smem_bytes"] <= 227 * 1024
+    exact = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL, precision=_lib.PREC_FP64_EXACT))
+    assert exact.info()["variant_ms"][4] == -1.0  # no three-blocks-per-SM tile kernel in exact mode
 
 
 # ------------------------------------------------------------------ FP32_FLUX mode
