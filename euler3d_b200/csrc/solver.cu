@@ -122,16 +122,34 @@ __device__ __forceinline__ void coeff_body(const CoeffArgs &a, double (*terms)[k
             __syncthreads();
         }
     } else {
-        // fixed-shape tree: strided per-thread sums, then a pairwise tree (deterministic)
+        // fixed-shape tree: strided per-thread sums over wall faces t, t + T, t + 2T, ... in that
+        // order (their loads issued four faces at a time), then a pairwise tree (deterministic)
+        constexpr int U = 4;
         double acc[6] = {0, 0, 0, 0, 0, 0};
-        for (int i = threadIdx.x; i < a.n_wall; i += kCoeffThreads) {
-            double p = wall_pressure(a, a.cell[i]);
-            double cp = a.cp_factor * (p - a.p_inf);
+        for (int base = threadIdx.x; base < a.n_wall; base += U * kCoeffThreads) {
+            double p[U], sv[U][3], ce[U][3];
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                double coeff = a.svec[3 * i + k] * cp * a.cref / a.sref;
-                acc[k] += coeff;
-                acc[3 + k] += coeff * a.center[3 * i + k];
+            for (int u = 0; u < U; u++) {
+                const int i = base + u * kCoeffThreads;
+                if (i < a.n_wall) {
+                    p[u] = wall_pressure(a, a.cell[i]);
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        sv[u][k] = a.svec[3 * i + k];
+                        ce[u][k] = a.center[3 * i + k];
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (base + u * kCoeffThreads >= a.n_wall) break;
+                const double cp = a.cp_factor * (p[u] - a.p_inf);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const double coeff = sv[u][k] * cp * a.cref / a.sref;
+                    acc[k] += coeff;
+                    acc[3 + k] += coeff * ce[u][k];
+                }
             }
         }
 #pragma unroll

@@ -276,15 +276,15 @@ struct Solver {
         ghost_copy.release();
     }
 
-    // Without tuning: the face-tile kernel (three blocks per SM in FP32_FLUX mode), or the gather
-    // kernel when the mesh does not fit the tiles.
+    // Without tuning: the face-tile kernel (three blocks per SM in FP64 and FP32_FLUX modes), or the
+    // gather kernel when the mesh does not fit the tiles.
     void use_default_variant() {
         for (auto &m : variant_ms) m = -1.0f;
         if (f32) {
             variant = 3;
             prepare_tile_f32(tile32_smem);
         } else if (tiles_ok) {
-            variant = 2;
+            variant = prm.precision == E3D_PREC_FP64 ? 4 : 2;
             if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
             else prepare_tile_fast(tile_smem, pipe_smem);
         } else {

@@ -888,8 +888,8 @@ __device__ __forceinline__ int2 batch_stage_args(const BatchStage &bs, StageArgs
     return e;
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(kStageThreads, 2) tile_batch_kernel(BatchStage bs) {
+template <bool EXACT, int MINB>
+__global__ void __launch_bounds__(kStageThreads, MINB) tile_batch_kernel(BatchStage bs) {
     if ((int)blockIdx.x >= *bs.n_entries) return;  // uniform across the block
     __shared__ __align__(16) StageArgs sa;
     const int2 e = batch_stage_args(bs, &sa);

@@ -11,11 +11,11 @@ void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<false>, pipe_smem_bytes);
 }
 
-void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false>, smem_bytes); }
+void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false, 2>, smem_bytes); }
 
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_batch_kernel<false><<<grid, kStageThreads, smem_bytes, s>>>(bs);
+    tile_batch_kernel<false, 2><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;

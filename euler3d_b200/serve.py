@@ -328,8 +328,11 @@ def compare(requests: Sequence[SolveRequest], precision: int = _lib.PREC_FP64, i
         ok = [b for b in base if b.status == _lib.E3D_OK and by[b.rid].status == _lib.E3D_OK]
         dl = [abs(b.cl - by[b.rid].cl) / max(abs(b.cl), 1e-3) for b in ok]
         dd = [abs(b.cd - by[b.rid].cd) / max(abs(b.cd), 1e-3) for b in ok]
-        out["same_outcome"] = all((b.status, b.stop_reason) == (by[b.rid].status, by[b.rid].stop_reason)
-                                  for b in base)
+        mism = [b for b in base if (b.status, b.stop_reason) != (by[b.rid].status, by[b.rid].stop_reason)]
+        out["same_outcome"] = not mism
+        out["outcome_mismatches"] = [{"rid": b.rid, "cells": b.cells, "plain": [b.status, b.stop_reason, b.iterations],
+                                      "served": [by[b.rid].status, by[b.rid].stop_reason, by[b.rid].iterations]}
+                                     for b in mism]
         out["max_rel_diff_cl"] = max(dl) if dl else None
         out["max_rel_diff_cd"] = max(dd) if dd else None
         out["max_iteration_diff"] = max(abs(b.iterations - by[b.rid].iterations) for b in base) if base else None
