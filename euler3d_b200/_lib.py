@@ -18,6 +18,7 @@ PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
 ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE, KERNEL_TILE_B3 = 0, 1, 2, 3, 4, 5
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS = 0, 1, 2
+INTEGRATOR_RK5, INTEGRATOR_EULER = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -44,7 +45,7 @@ class FlowParams(C.Structure):
                 ("cl_axis", C.c_int32), ("cl_sign", C.c_int32), ("cd_axis", C.c_int32), ("cd_sign", C.c_int32),
                 ("cm_axis", C.c_int32), ("cm_sign", C.c_int32), ("scheme", C.c_int32), ("precision", C.c_int32),
                 ("ordering", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
-                ("no_autotune", C.c_int32)]
+                ("no_autotune", C.c_int32), ("integrator", C.c_int32), ("residual_smoothing", C.c_int32)]
 
 
 class RunParams(C.Structure):

@@ -88,6 +88,14 @@ public:
         p.scheme = config.getSolverScheme() == E3D::Parser::SimConfig::SolverScheme::AUSM ? E3D_SCHEME_AUSM : E3D_SCHEME_ROE;
         p.precision = precision;
         p.ordering = E3D_ORDER_SPATIAL;
+        // TIME_INTEGRATION= (EulerSolver's constructor, src/solver/EulerSolver.cpp:49-56); the
+        // implicit scheme is a stub there that never updates the state
+        switch (config.getTemporalScheme()) {
+            case E3D::Parser::SimConfig::TemporalScheme::RK5: p.integrator = E3D_INTEGRATOR_RK5; break;
+            case E3D::Parser::SimConfig::TemporalScheme::EXPLICIT_EULER: p.integrator = E3D_INTEGRATOR_EULER; break;
+            default: throw std::runtime_error("TIME_INTEGRATION= 1 (implicit Euler) is not supported on the GPU");
+        }
+        p.residual_smoothing = config.getResidualSmoothing() ? 1 : 0;
         check(e3d_solver_create(&d, &p, &_solver), "e3d_solver_create");
         if ((size_t)e3d_solver_state_size(_solver) != flow.Getrho().size())
             throw std::runtime_error("every boundary face needs a wall, farfield or sym marker");

@@ -342,6 +342,8 @@ e3d_status e3d_batch_add(e3d_batch *batch, e3d_solver *solver, const e3d_run_par
             throw Error(E3D_ERR_INVALID_ARG, "solver precision differs from the batch's members");
         if (!S->tiles_ok)
             throw Error(E3D_ERR_INVALID_ARG, "the solver's mesh does not fit the face-tile kernel a batch runs");
+        if (S->euler() || S->smoothing)
+            throw Error(E3D_ERR_INVALID_ARG, "batch members run RK5 without residual smoothing");
         E3D_CUDA(cudaSetDevice(B->device));
         E3D_CUDA(cudaStreamSynchronize(S->stream));  // the solver's own pending work (state uploads)
         begin_run(S, rp, B->stream);

@@ -221,6 +221,71 @@ __global__ void control_gather_kernel(Control *const *__restrict__ ctl, const in
     for (int i = threadIdx.x; i < (int)(sizeof(Control) / 4); i += blockDim.x) dst[i] = src[i];
 }
 
+// One Jacobi pass of EulerSolver::smoothResiduals (src/solver/EulerSolver.cpp:483-518), one thread
+// per cell:  out_c = (r0_c + sum_j 0.25 last_j) / (1 + 0.25 n_faces(c)), the sum over interior
+// neighbours in element2element order, in the reference's operation order.  The reference's loop
+// ends after at most two passes (its difference vector is cleared after the first pass, so the
+// second measures no change): the first pass records its largest change (and any NaN, on which the
+// reference exits the process); the second pass runs only if that change is above 1e-16 and
+// otherwise copies the first pass's result, so the update always reads the second buffer.
+constexpr int kSmoothThreads = 256;
+
+__global__ void __launch_bounds__(kSmoothThreads) smooth_kernel(SmoothArgs a) {
+    if (a.ctl->done) return;  // uniform across the grid
+    const int c = blockIdx.x * kSmoothThreads + threadIdx.x;
+    const size_t st = (size_t)a.stride;
+    if (a.pass == 1) {
+        if (a.flags[1]) {  // NaN in the first pass: stop the run as non-finite
+            if (c == 0) {
+                a.ctl->nonfinite = 1;
+                a.ctl->stop_reason = E3D_STOP_MAX_ITER;
+                a.ctl->done = 1;
+            }
+            return;
+        }
+        if (!(__longlong_as_double((long long)a.flags[0]) > 1e-16)) {
+            if (c < a.n_cells)
+                for (int q = 0; q < 5; q++) a.out[q * st + c] = a.last[q * st + c];
+            return;
+        }
+    }
+    double m = 0.0;
+    int bad = 0;
+    if (c < a.n_cells) {
+        double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = a.nb_ptr[c]; k < a.nb_ptr[c + 1]; k++) {
+            const int j = a.nb[k];
+#pragma unroll
+            for (int q = 0; q < 5; q++) sum[q] += a.last[q * st + j] * 0.25;
+        }
+        const double d = a.den[c];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            const double v = (a.r0[q * st + c] + sum[q]) / d;
+            a.out[q * st + c] = v;
+            const double ch = fabs(a.last[q * st + c] - v);
+            if (isnan(ch)) bad = 1;
+            else if (ch > m) m = ch;
+        }
+    }
+    if (a.pass != 0) return;
+    // block maximum of the change (non-negative doubles order like their bit patterns)
+    __shared__ double sm[kSmoothThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kSmoothThreads / 32; w++) m = fmax(m, sm[w]);
+        m = fmax(m, sm[0]);
+        atomicMax(&a.flags[0], (unsigned long long)__double_as_longlong(m));
+        if (bad) atomicOr(&a.flags[1], 1ull);
+    }
+}
+
+void launch_smooth(const SmoothArgs &a, cudaStream_t s) {
+    smooth_kernel<<<(a.n_cells + kSmoothThreads - 1) / kSmoothThreads, kSmoothThreads, 0, s>>>(a);
+}
+
 void launch_finalize(const FinalizeArgs &f, cudaStream_t s) { finalize_kernel<<<1, kReduceThreads, 0, s>>>(f); }
 void launch_coeff(const CoeffArgs &c, cudaStream_t s) { coeff_kernel<<<1, kCoeffThreads, 0, s>>>(c); }
 void launch_finalize_batch(const FinalizeArgs *f, const int *n_members, int grid, cudaStream_t s) {
@@ -582,6 +647,12 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
         throw Error(E3D_ERR_INVALID_ARG, "flow parameters out of range (gamma > 1, cfl > 0, mach >= 0, cref, sref != 0)");
     for (int ax : {p->cl_axis, p->cd_axis, p->cm_axis})
         if (ax < 0 || ax > 2) throw Error(E3D_ERR_INVALID_ARG, "coefficient axis must be 0, 1 or 2");
+    if (p->integrator != E3D_INTEGRATOR_RK5 && p->integrator != E3D_INTEGRATOR_EULER)
+        throw Error(E3D_ERR_INVALID_ARG, "unknown integrator (E3D_INTEGRATOR_RK5 or E3D_INTEGRATOR_EULER)");
+    if (p->residual_smoothing != 0 && p->residual_smoothing != 1)
+        throw Error(E3D_ERR_INVALID_ARG, "residual_smoothing must be 0 or 1");
+    if (p->precision == E3D_PREC_FP32_FLUX && (p->integrator != E3D_INTEGRATOR_RK5 || p->residual_smoothing))
+        throw Error(E3D_ERR_INVALID_ARG, "FP32_FLUX mode runs RK5 without residual smoothing only");
 
     int ndev = 0;
     E3D_CUDA(cudaGetDeviceCount(&ndev));
@@ -777,6 +848,31 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     }
     S->w0_stride = (N + 31) / 32 * 32;
     S->w0.alloc(5 * (size_t)S->w0_stride);
+    if (p->residual_smoothing) {
+        // interior neighbours of each device cell in the reference's element2face order (which is
+        // its element2element order, src/connectivity/Connectivity.cpp:184-218), and 1 + 0.25 n
+        // with n counting every face (EulerSolver.cpp:500-504)
+        std::vector<int> nptr(N + 1, 0), nbl;
+        std::vector<double> den(N);
+        nbl.reserve(d->cell2face_ptr[N]);
+        for (int c = 0; c < N; c++) {
+            const int o = new2old[c];
+            for (int k = d->cell2face_ptr[o]; k < d->cell2face_ptr[o + 1]; k++) {
+                const int f = d->cell2face[k];
+                const int j = d->face2cell[2 * f] == o ? d->face2cell[2 * f + 1] : d->face2cell[2 * f];
+                if (j < N) nbl.push_back(old2new[j]);
+            }
+            nptr[c + 1] = (int)nbl.size();
+            den[c] = 1 + (d->cell2face_ptr[o + 1] - d->cell2face_ptr[o]) * 0.25;
+        }
+        S->smoothing = true;
+        S->nb_ptr.upload(nptr, s);
+        S->nb.upload(nbl, s);
+        S->den.upload(den, s);
+        S->rbuf.alloc(3 * 5 * (size_t)S->w0_stride);
+        S->smooth_flags.alloc(2);
+        E3D_CUDA(cudaMemsetAsync(S->rbuf.p, 0, S->rbuf.n * sizeof(double), s));
+    }
     S->ecell.alloc(N);
     S->minit.alloc(N);
     S->ghost.alloc(8 * (size_t)std::max(G, 1));
@@ -1073,7 +1169,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
             int launched_iters = 0;
             while (max_iter > 0) {
                 E3D_CUDA(cudaGraphLaunch(S->graph, S->stream));
-                launches += 7LL * every;
+                launches += (int64_t)S->kernels_per_iteration() * every;
                 launched_iters += every;
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
                 E3D_CUDA(cudaStreamSynchronize(S->stream));
@@ -1082,32 +1178,32 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
                     throw Error(E3D_ERR_TIMEOUT, "run did not reach its stop condition");
             }
         } else {
-            // direct launches, an event pair around every stage kernel
-            static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+            // direct launches, an event pair around every stage (its kernels)
             if (!S->prof_ev[0]) {
                 for (auto &e : S->prof_ev) E3D_CUDA(cudaEventCreate(&e));
             }
             E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
             int b = 0;
             for (int it = 0; it < max_iter; it++) {
-                for (int st_i = 0; st_i < 5; st_i++) {
+                const int ns = S->n_stages();
+                for (int st_i = 0; st_i < ns; st_i++) {
                     E3D_CUDA(cudaEventRecord(S->prof_ev[2 * st_i], S->stream));
-                    S->launch_stage(S->stage_args(b, alphas[st_i], st_i == 0, st_i == 4));
+                    S->enqueue_stage(b, st_i, S->partials.p);
                     E3D_CUDA(cudaEventRecord(S->prof_ev[2 * st_i + 1], S->stream));
                     b = 1 - b;
                 }
                 launch_finalize(S->finalize_args(S->partials.p, S->hist.p), S->stream);
                 launch_coeff(S->coeff_args(b, 1, nullptr), S->stream);
                 E3D_CUDA(cudaGetLastError());
-                launches += 7;
+                launches += S->kernels_per_iteration();
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
                 E3D_CUDA(cudaStreamSynchronize(S->stream));
-                for (int st_i = 0; st_i < 5; st_i++) {
+                for (int st_i = 0; st_i < ns; st_i++) {
                     float ms = 0.f;
                     E3D_CUDA(cudaEventElapsedTime(&ms, S->prof_ev[2 * st_i], S->prof_ev[2 * st_i + 1]));
                     stage_ms += ms;
                 }
-                stage_launches += 5;
+                stage_launches += ns;
                 if (S->ctl_host->done) break;
             }
         }
@@ -1177,6 +1273,8 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
             throw Error(E3D_ERR_INVALID_ARG, "mesh of " + std::to_string(S->N) + " cells exceeds the no-alloc limit of " +
                                                  std::to_string(kNoAllocMaxBlocks * kStageThreads) + " cells");
         if (rp->stage_kernel != 0) throw Error(E3D_ERR_INVALID_ARG, "the no-alloc run uses the handle's stage kernel");
+        if (S->euler() || S->smoothing)
+            throw Error(E3D_ERR_INVALID_ARG, "the no-alloc run supports RK5 without residual smoothing only");
         double *partials = noalloc_scratch(S->device);
         double *hist = partials + kNoAllocMaxBlocks;
         // the history region starts cleared, so no entry of an earlier call can be read back

@@ -24,6 +24,8 @@ constexpr int kStageVariants = 5;
 
 constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
+void launch_update_exact(const StageArgs &a, cudaStream_t s);
+void launch_update_fast(const StageArgs &a, cudaStream_t s);
 void prepare_batch_exact(size_t smem_bytes);
 void prepare_batch_fast(size_t smem_bytes);
 void prepare_batch_f32(size_t smem_bytes);
@@ -57,12 +59,28 @@ struct FinalizeArgs {
     Control *ctl;
 };
 
+// Residual smoothing (EulerSolver::smoothResiduals, src/solver/EulerSolver.cpp:483-518): one Jacobi
+// pass over every cell.
+struct SmoothArgs {
+    int n_cells, stride;                 // stride: row stride of the [5 x stride] residual arrays
+    const int *__restrict__ nb_ptr;      // interior neighbours of each cell, element2face order
+    const int *__restrict__ nb;
+    const double *__restrict__ den;      // 1 + 0.25 x (faces of the cell, ghosts included)
+    const double *__restrict__ r0;       // the stage's residual
+    const double *__restrict__ last;     // this pass's input
+    double *__restrict__ out;
+    unsigned long long *flags;           // [0] largest change of the first pass (bits), [1] NaN seen
+    Control *ctl;
+    int pass;                            // 0 first pass, 1 second pass
+};
+
 // Kernels of solver.cu, launched through these.
 void launch_finalize(const FinalizeArgs &f, cudaStream_t s);
 void launch_coeff(const CoeffArgs &c, cudaStream_t s);
 void launch_finalize_batch(const FinalizeArgs *f, const int *n_members, int grid, cudaStream_t s);
 void launch_coeff_batch(const CoeffArgs *c, const int *n_members, int parity, int grid, cudaStream_t s);
 void launch_control_gather(Control *const *ctl, const int *n_members, Control *out, int grid, cudaStream_t s);
+void launch_smooth(const SmoothArgs &a, cudaStream_t s);
 
 template <typename T>
 struct DevBuf {
@@ -118,6 +136,12 @@ struct Solver {
     DevBuf<double4> fgeo, cgeo;
     DevBuf<double2> q[2];
     DevBuf<double> w0, ecell, minit, ghost, partials, staging, wall_svec, wall_center, hist, scratch;
+    // residual smoothing: interior neighbours (element2face order), denominators, residual arrays
+    // r0 (the stage's residual), r1, r2 (after the first / second Jacobi pass), pass flags
+    bool smoothing = false;
+    DevBuf<int> nb_ptr, nb;
+    DevBuf<double> den, rbuf;
+    DevBuf<unsigned long long> smooth_flags;
     Control *ctl = nullptr;        // device
     Control *ctl_host = nullptr;   // pinned mirror
     int cur = 0;                   // q buffer holding the current state
@@ -151,7 +175,10 @@ struct Solver {
         q[0].release();
         q[1].release();
         DevBuf<double> *db[] = {&w0, &ecell, &minit, &ghost, &partials, &staging, &wall_svec, &wall_center, &hist,
-                                &scratch};
+                                &scratch, &den, &rbuf};
+        nb_ptr.release();
+        nb.release();
+        smooth_flags.release();
         for (auto *b : db) b->release();
         if (ctl) cudaFree(ctl);
         if (ctl_host) cudaFreeHost(ctl_host);
@@ -167,7 +194,8 @@ struct Solver {
                (int64_t)tile_rec32_off.n * 8 +
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
-                         hist.n + scratch.n) * 8 + (int64_t)sizeof(Control);
+                         hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n) * 8 +
+               (int64_t)(nb_ptr.n + nb.n) * 4 + (int64_t)sizeof(Control);
     }
 
     StageArgs stage_args(int in_buf, double alpha, int first, int last) {
@@ -213,6 +241,9 @@ struct Solver {
         a.tile_rec32 = reinterpret_cast<const char *>(tile_rec32.p);
         a.tile_rec32_off = tile_rec32_off.p;
         a.cgeo32 = cgeo32.p;
+        a.integrator = prm.integrator;
+        a.split = 0;
+        a.r_dev = nullptr;
         return a;
     }
 
@@ -324,17 +355,55 @@ struct Solver {
         return FinalizeArgs{part, n_blocks, (double)N, h, ctl};
     }
 
-    // One RK5 iteration (src/solver/EulerSolver.cpp:84-153) starting from q[in_buf]; returns launches.
-    int enqueue_iteration(int in_buf) {
+    bool euler() const { return prm.integrator == E3D_INTEGRATOR_EULER; }
+    // Stages per iteration (RK5: 5; explicit Euler: 1) and kernels per stage and per iteration.
+    int n_stages() const { return euler() ? 1 : 5; }
+    int kernels_per_stage() const { return smoothing ? 4 : 1; }
+    int kernels_per_iteration() const { return n_stages() * kernels_per_stage() + 2; }
+
+    // Stage s of an iteration from q[b] (EulerSolver::RungeKutta, src/solver/EulerSolver.cpp:425-472,
+    // or EulerSolver::EulerExplicit, :419-423).  Without smoothing one fused kernel; with it the
+    // residual phase writes R, two Jacobi passes smooth it (EulerSolver::smoothResiduals, :483-518,
+    // called by Run() :91-93 for the first stage and by RungeKutta :456-458 for the others) and the
+    // update kernel applies it.
+    void enqueue_stage(int b, int s, double *part) {
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+        StageArgs a = stage_args(b, euler() ? 1.0 : alphas[s], s == 0, euler() || s == 4);
+        a.partials = part;
+        if (!smoothing) {
+            launch_stage(a);
+            return;
+        }
+        const size_t n5 = 5 * (size_t)w0_stride;
+        double *r0 = rbuf.p, *r1 = rbuf.p + n5, *r2 = rbuf.p + 2 * n5;
+        StageArgs ar = a;
+        ar.split = 1;
+        ar.last_stage = 0;
+        ar.r_dev = r0;
+        launch_stage(ar);
+        E3D_CUDA(cudaMemsetAsync(smooth_flags.p, 0, 2 * sizeof(unsigned long long), stream));
+        SmoothArgs sa{N, w0_stride, nb_ptr.p, nb.p, den.p, r0, r0, r1, smooth_flags.p, ctl, 0};
+        launch_smooth(sa, stream);
+        sa.last = r1;
+        sa.out = r2;
+        sa.pass = 1;
+        launch_smooth(sa, stream);
+        a.r_dev = r2;
+        if (prm.precision == E3D_PREC_FP64_EXACT) launch_update_exact(a, stream);
+        else launch_update_fast(a, stream);
+    }
+
+    // One iteration of EulerSolver::Run (src/solver/EulerSolver.cpp:84-153) starting from q[in_buf];
+    // returns the kernels launched.
+    int enqueue_iteration(int in_buf) {
         int b = in_buf;
-        for (int s = 0; s < 5; s++) {
-            launch_stage(stage_args(b, alphas[s], s == 0, s == 4));
+        for (int s = 0; s < n_stages(); s++) {
+            enqueue_stage(b, s, partials.p);
             b = 1 - b;
         }
         launch_finalize(finalize_args(partials.p, hist.p), stream);
         launch_coeff(coeff_args(b, 1, nullptr), stream);
-        return 7;
+        return kernels_per_iteration();
     }
 
     void build_graph(int iters) {

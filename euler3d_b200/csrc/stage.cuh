@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "euler3d_b200.h"
+
 namespace e3d {
 
 enum : int { TAG_LEFT = 0, TAG_RIGHT = 1, TAG_WALL = 2, TAG_SYM = 3, TAG_FAR = 4, TAG_FROZEN = 5 };
@@ -96,6 +98,10 @@ struct StageArgs {
     const char *__restrict__ tile_rec32;
     const long long *__restrict__ tile_rec32_off;
     const float4 *__restrict__ cgeo32;
+    int integrator;                  // E3D_INTEGRATOR_RK5 or E3D_INTEGRATOR_EULER (uniform)
+    int split;                       // residual phase of a split stage: write R to r_dev, no update
+    double *__restrict__ r_dev;      // [5 x w0_stride] residual of a split stage (device order); the
+                                     // update phase reads the smoothed residual from here
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -488,9 +494,27 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         a.dt_out[o] = dt;
         return 0.0;
     }
-    // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
+    if (a.split) {  // residual smoothing runs between this residual and the update
+        const size_t st = (size_t)a.w0_stride;
+#pragma unroll
+        for (int k = 0; k < 5; k++) a.r_dev[k * st + c] = R[k];
+        return 0.0;
+    }
     double W[5];
-    if (EXACT) {
+    if (a.integrator == E3D_INTEGRATOR_EULER) {
+        // ExplicitEuler (src/solver/TimeIntegration.cpp:78-91) and FlowField::Update
+        // (src/solver/FlowField.cpp:103-117): W += R * (-dt / V), W the carried conservative state
+        if (EXACT) {
+            const double coeff = -dt / cg.w;
+#pragma unroll
+            for (int k = 0; k < 5; k++) W[k] = W0[k] + R[k] * coeff;
+        } else {
+            const double coef = a.cfl * rcp_nr(lam);  // dt / V
+#pragma unroll
+            for (int k = 0; k < 5; k++) W[k] = W0[k] - coef * R[k];
+        }
+    } else if (EXACT) {
+        // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
 #pragma unroll
         for (int k = 0; k < 5; k++) W[k] = W0[k] - a.alpha * dt * R[k] / cg.w;
     } else {
@@ -520,8 +544,14 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
     }
     store_prim(a.qout, c, s);
     if (!a.last_stage) return 0.0;
-    // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
     const size_t st = (size_t)a.w0_stride;
+    if (a.integrator == E3D_INTEGRATOR_EULER) {  // the conservative state itself carries over
+#pragma unroll
+        for (int k = 0; k < 5; k++) a.w0[k * st + c] = W[k];
+        a.ecell[c] = E;
+        return R[0] * R[0];
+    }
+    // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
     a.w0[0 * st + c] = s.rho;
     a.w0[1 * st + c] = s.u * s.rho;
     a.w0[2 * st + c] = s.v * s.rho;
@@ -988,6 +1018,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         __syncthreads();  // buffer cur (with its fluxes) and sq are free again
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ---- update phase of a split stage
+// One thread per cell: the time step and the update of finish_cell from the residual in r_dev
+// (smoothed between the residual phase and this one).  Blocks of kStageThreads cells, so the RMS
+// partials line up with those of the stage kernels.
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageThreads) update_kernel(StageArgs a) {
+    if (a.ctl->done) return;  // uniform across the grid
+    const int c = blockIdx.x * kStageThreads + threadIdx.x;
+    double r2 = 0.0;
+    if (c < a.n_cells) {
+        const Prim me = load_prim(a.qin, c);
+        const size_t st = (size_t)a.w0_stride;
+        double R[5], W0[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            R[k] = a.r_dev[k * st + c];
+            W0[k] = a.w0[k * st + c];
+        }
+        const double r_me = EXACT ? 0.0 : rsqrt_nr(a.gamma * me.p * me.rho);
+        r2 = finish_cell<EXACT>(a, c, me, r_me, R, W0, a.cgeo[c]);
+    }
+    if (a.last_stage) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
 // Dynamic shared memory of tile_kernel (buffers = 1) and tile_pipe_kernel (buffers = 2).

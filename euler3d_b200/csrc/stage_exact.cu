@@ -13,6 +13,11 @@ void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes) {
 
 void prepare_batch_exact(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<true, 2>, smem_bytes); }
 
+// Update phase of a split stage (residual smoothing between residual and update).
+void launch_update_exact(const StageArgs &a, cudaStream_t s) {
+    update_kernel<true><<<(a.n_cells + kStageThreads - 1) / kStageThreads, kStageThreads, 0, s>>>(a);
+}
+
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
     tile_batch_kernel<true, 2><<<grid, kStageThreads, smem_bytes, s>>>(bs);

@@ -371,7 +371,8 @@ class CaseConfig:
     max_iter: int = 100
     sampling: int = 1
     scheme: int = 0
-    time_integration: int = 2
+    time_integration: int = 2     # TIME_INTEGRATION=: 0 explicit Euler, 2 RK5
+    residual_smoothing: int = 0   # RESIDUAL_SMOOTHING=
     orientation_cl: int = 2
     orientation_cd: int = 0
     ref_point: Tuple[float, float, float] = (0.25, 0.0, 0.0)
@@ -409,7 +410,7 @@ def write_e3d(cfg: CaseConfig, path: str, par_pattern: str, output_file: str, n_
         "SPECIFIC_HEAT= 1004.7",
         f"SCHEME= {cfg.scheme}",
         f"TIME_INTEGRATION= {cfg.time_integration}",
-        "RESIDUAL_SMOOTHING= 0",
+        f"RESIDUAL_SMOOTHING= {cfg.residual_smoothing}",
         f"CFL= {cfg.cfl!r}",
         f"MIN_RESIDUAL= {cfg.min_residual!r}",
         f"MIN_AEROCOEFF_ERROR= {cfg.min_aerocoeff_error!r}",

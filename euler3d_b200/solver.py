@@ -154,6 +154,8 @@ class FlowConfig:
     precision: int = _lib.PREC_FP64
     ordering: int = _lib.ORDER_NATIVE
     device: int = 0
+    integrator: int = _lib.INTEGRATOR_RK5   # TIME_INTEGRATION= 2 (RK5) or 0 (INTEGRATOR_EULER)
+    smoothing: bool = False                  # RESIDUAL_SMOOTHING=
 
     @staticmethod
     def orientation(cl_code: int, cd_code: int):
@@ -199,6 +201,7 @@ class EulerSolver:
         p.scheme, p.precision, p.ordering, p.device = flow.scheme, flow.precision, flow.ordering, flow.device
         p.stream = stream
         p.no_autotune = 0 if autotune else 1
+        p.integrator, p.residual_smoothing = flow.integrator, int(bool(flow.smoothing))
         h = C.c_void_p()
         check(lib.e3d_solver_create(C.byref(self._desc.c), C.byref(p), C.byref(h)))
         self._h = h

@@ -56,6 +56,14 @@ enum { E3D_PREC_FP64_EXACT = 0, E3D_PREC_FP64 = 1, E3D_PREC_FP32_FLUX = 2 };
  * (spatially compact groups of cells, which the face-tile kernel needs). */
 enum { E3D_ORDER_NATIVE = 0, E3D_ORDER_RCM = 1, E3D_ORDER_SPATIAL = 2 };
 
+/* Time integration (the reference's TIME_INTEGRATION= key, src/parser/SimConfig.cpp:130-148, and
+ * EulerSolver's constructor, src/solver/EulerSolver.cpp:49-56): RK5 is TIME_INTEGRATION= 2
+ * (EulerSolver::RungeKutta, :425-472); EULER is TIME_INTEGRATION= 0, explicit Euler
+ * (EulerSolver::EulerExplicit, :419-423: W += R * (-dt / V) on the carried conservative state).
+ * TIME_INTEGRATION= 1 (EulerImplicit, :474-480) never updates the state in the reference and has
+ * no counterpart here. */
+enum { E3D_INTEGRATOR_RK5 = 0, E3D_INTEGRATOR_EULER = 1 };
+
 /* Why e3d_solver_run stopped (the exits of EulerSolver::Run, src/solver/EulerSolver.cpp:100-152). */
 enum { E3D_STOP_MAX_ITER = 0, E3D_STOP_RESIDUAL = 1, E3D_STOP_COEFFICIENTS = 2 };
 
@@ -140,6 +148,10 @@ typedef struct e3d_flow_params {
 	void *stream;                     /* cudaStream_t to run on, or NULL for a library-owned stream */
 	int32_t no_autotune;              /* 1: skip the creation-time timing of the stage-kernel variants
 	                                     and use the face-tile kernel (what a batch runs anyway) */
+	int32_t integrator;               /* E3D_INTEGRATOR_* (TIME_INTEGRATION=) */
+	int32_t residual_smoothing;       /* RESIDUAL_SMOOTHING=: EulerSolver::smoothResiduals
+	                                     (src/solver/EulerSolver.cpp:483-518) on every residual that
+	                                     updates the state; FP64 and FP64_EXACT only */
 } e3d_flow_params;
 
 typedef struct e3d_solver e3d_solver;

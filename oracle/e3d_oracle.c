@@ -324,35 +324,110 @@ void orc_time_step(const orc_mesh *m, const orc_flow *fl, const orc_state *s, do
 	}
 }
 
+/* Primitive recovery of FlowField::Update / updateWRungeKutta (src/solver/FlowField.cpp:118-127,
+ * :150-159) from the conservative state w of cell c. */
+static void set_primitives(const orc_flow *fl, orc_state *s, int c, const double w[5]) {
+	const double g = fl->gamma;
+	double rho = w[0];
+	double u = w[1] / rho, v = w[2] / rho, ww = w[3] / rho, E = w[4] / rho;
+	double q2 = u * u + v * v + ww * ww;
+	double p = (g - 1) * rho * (E - q2 / 2.0);
+	s->rho[c] = rho;
+	s->u[c] = u;
+	s->v[c] = v;
+	s->w[c] = ww;
+	s->E[c] = E;
+	s->p[c] = p;
+	s->H[c] = E + (p / rho);
+	s->M[c] = sqrt(g * (p / rho)) / sqrt(q2);
+}
+
 /* One stage: W = W0 - alpha*dt*R/V followed by FlowField::updateWRungeKutta's primitive recovery,
  * src/solver/EulerSolver.cpp:441-450 / :461-470 and src/solver/FlowField.cpp:140-171. */
 static void rk_update(const orc_mesh *m, const orc_flow *fl, orc_state *s, const double *W0, const double *R,
                       const double *dt, double alpha) {
-	const double g = fl->gamma;
 	for (int c = 0; c < m->n_cells; c++) {
 		double vol = m->cell_volume[c];
 		double w[5];
 		for (int k = 0; k < 5; k++) w[k] = W0[5 * (size_t) c + k] - alpha * dt[c] * R[5 * (size_t) c + k] / vol;
-		double rho = w[0];
-		double u = w[1] / rho, v = w[2] / rho, ww = w[3] / rho, E = w[4] / rho;
-		double q2 = u * u + v * v + ww * ww;
-		double p = (g - 1) * rho * (E - q2 / 2.0);
-		s->rho[c] = rho;
-		s->u[c] = u;
-		s->v[c] = v;
-		s->w[c] = ww;
-		s->E[c] = E;
-		s->p[c] = p;
-		s->H[c] = E + (p / rho);
-		s->M[c] = sqrt(g * (p / rho)) / sqrt(q2);
+		set_primitives(fl, s, c, w);
+	}
+}
+
+/* EulerSolver::smoothResiduals, src/solver/EulerSolver.cpp:483-518.  The neighbours of cell c are
+ * the other cells of its faces in element2face order, which is the reference's element2element
+ * order (both are filled per local face, src/connectivity/Connectivity.cpp:184-218); ghost
+ * neighbours count in the denominator but not in the sum.
+ * The reference's loop runs at most two passes: each pass ends with diff.clear() (:514), so the
+ * next pass measures its changes over an empty vector (its std::transform writes into the cleared
+ * vector's storage, :505), finds error = 0 and leaves the loop.  One pass if the first pass's
+ * largest change is <= 1e-16, otherwise exactly two; only the first pass is checked for NaN. */
+static void smooth_pass(const orc_mesh *m, const double *orig, const double *last, double *R) {
+	const double epsilon = 0.25;
+	for (int c = 0; c < m->n_cells; c++) {
+		double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+		const int n_surr = m->cell2face_ptr[c + 1] - m->cell2face_ptr[c];
+		for (int k = m->cell2face_ptr[c]; k < m->cell2face_ptr[c + 1]; k++) {
+			const int f = m->cell2face[k];
+			const int j = m->face2cell[2 * f] == c ? m->face2cell[2 * f + 1] : m->face2cell[2 * f];
+			if (j < m->n_cells)
+				for (int q = 0; q < 5; q++) sum[q] += last[5 * (size_t) j + q] * epsilon;
+		}
+		for (int q = 0; q < 5; q++) R[5 * (size_t) c + q] = (orig[5 * (size_t) c + q] + sum[q]) / (1 + n_surr * epsilon);
+	}
+}
+
+long long orc_smooth_residuals(const orc_mesh *m, double *R) {
+	const size_t n5 = 5 * (size_t) m->n_cells;
+	double *orig = (double *) malloc(sizeof(double) * (n5 ? n5 : 1));
+	double *last = (double *) malloc(sizeof(double) * (n5 ? n5 : 1));
+	if (!orig || !last) {
+		free(orig);
+		free(last);
+		return -1;
+	}
+	memcpy(orig, R, sizeof(double) * n5);
+	memcpy(last, R, sizeof(double) * n5);
+	smooth_pass(m, orig, last, R);
+	double error = 0.0;
+	for (size_t i = 0; i < n5; i++) {
+		double d = fabs(last[i] - R[i]);
+		if (isnan(d)) {
+			free(orig);
+			free(last);
+			return -1;
+		}
+		if (d > error) error = d;
+	}
+	long long sweeps = 1;
+	if (error > 1e-16) {
+		memcpy(last, R, sizeof(double) * n5);
+		smooth_pass(m, orig, last, R);
+		sweeps = 2;
+	}
+	free(orig);
+	free(last);
+	return sweeps;
+}
+
+/* EulerSolver::EulerExplicit, src/solver/EulerSolver.cpp:419-423 (updateDeltaTime,
+ * TimeIntegration :369-374 with ExplicitEuler src/solver/TimeIntegration.cpp:78-91, updateW). */
+void orc_euler_explicit(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *W, const double *R, double *dt) {
+	orc_time_step(m, fl, s, dt);
+	for (int c = 0; c < m->n_cells; c++) {
+		double coeff = -dt[c] / m->cell_volume[c];
+		double *w = W + 5 * (size_t) c;
+		for (int q = 0; q < 5; q++) w[q] += R[5 * (size_t) c + q] * coeff;
+		set_primitives(fl, s, c, w);
 	}
 }
 
 /* EulerSolver::RungeKutta, src/solver/EulerSolver.cpp:425-472 */
-void orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *R, double *dt) {
+long long orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *R, double *dt) {
 	static const double alphas[4] = {0.1263, 0.2375, 0.4414, 1.0};
+	long long sweeps = 0;
 	double *W0 = (double *) malloc(sizeof(double) * 5 * (size_t) (m->n_cells > 0 ? m->n_cells : 1));
-	if (!W0) return;
+	if (!W0) return -1;
 	for (int c = 0; c < m->n_cells; c++) { /* W0 from the primitives, :431-438 */
 		double rho = s->rho[c];
 		W0[5 * (size_t) c + 0] = rho;
@@ -366,10 +441,19 @@ void orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double
 	for (int k = 0; k < 4; k++) {
 		orc_update_bc(m, fl, s);
 		orc_compute_residual(m, fl, s, R);
+		if (fl->smoothing) {
+			long long n = orc_smooth_residuals(m, R);
+			if (n < 0) {
+				free(W0);
+				return -1;
+			}
+			sweeps += n;
+		}
 		orc_time_step(m, fl, s, dt);
 		rk_update(m, fl, s, W0, R, dt, alphas[k]);
 	}
 	free(W0);
+	return sweeps;
 }
 
 double orc_rms(const orc_mesh *m, const double *R) {
@@ -411,19 +495,48 @@ void orc_aero_coefficients(const orc_mesh *m, const orc_flow *fl, const orc_stat
 int orc_run(const orc_mesh *m, const orc_flow *fl, orc_state *s, const orc_run_params *rp, orc_run_stats *st) {
 	double *R = (double *) malloc(sizeof(double) * 5 * (size_t) (m->n_cells > 0 ? m->n_cells : 1));
 	double *dt = (double *) malloc(sizeof(double) * (size_t) (m->n_cells > 0 ? m->n_cells : 1));
-	if (!R || !dt) {
+	double *W = NULL;
+	if (fl->integrator == 1) W = (double *) malloc(sizeof(double) * 5 * (size_t) (m->n_cells > 0 ? m->n_cells : 1));
+	if (!R || !dt || (fl->integrator == 1 && !W)) {
 		free(R);
 		free(dt);
+		free(W);
 		return -1;
 	}
 	memset(st, 0, sizeof *st);
+	if (W) /* FlowField's conservative arrays, FlowField::Initialize (src/solver/FlowField.cpp:86-95) */
+		for (int c = 0; c < m->n_cells; c++) {
+			double rho = s->rho[c];
+			W[5 * (size_t) c + 0] = rho;
+			W[5 * (size_t) c + 1] = rho * s->u[c];
+			W[5 * (size_t) c + 2] = rho * s->v[c];
+			W[5 * (size_t) c + 3] = rho * s->w[c];
+			W[5 * (size_t) c + 4] = rho * s->E[c];
+		}
 	int it = 0, counter = 0;
 	double cl = 0, cd = 0, cm = 0;
 	int sampling = rp->sampling > 0 ? rp->sampling : 1;
 	while (it < rp->max_iter) {
 		orc_update_bc(m, fl, s);
 		orc_compute_residual(m, fl, s, R);
-		orc_runge_kutta(m, fl, s, R, dt);
+		if (fl->smoothing) {
+			long long n = orc_smooth_residuals(m, R);
+			if (n < 0) {
+				st->converged = 3;
+				break;
+			}
+			st->smooth_sweeps += n;
+		}
+		if (fl->integrator == 1) {
+			orc_euler_explicit(m, fl, s, W, R, dt);
+		} else {
+			long long n = orc_runge_kutta(m, fl, s, R, dt);
+			if (n < 0) {
+				st->converged = 3;
+				break;
+			}
+			st->smooth_sweeps += n;
+		}
 		double rms = orc_rms(m, R);
 		if (rp->rms_history) rp->rms_history[st->n_rms] = rms;
 		st->n_rms++;
@@ -454,5 +567,6 @@ int orc_run(const orc_mesh *m, const orc_flow *fl, orc_state *s, const orc_run_p
 	st->cm = cm;
 	free(R);
 	free(dt);
+	free(W);
 	return 0;
 }

@@ -50,6 +50,8 @@ typedef struct {
 	double sref, cref, ref_point[3];
 	int cl_axis, cl_sign, cd_axis, cd_sign, cm_axis, cm_sign;
 	int scheme;                     /* 0 Roe (the reference), 1 AUSM (declared, never defined, in the reference) */
+	int integrator;                 /* 0 RK5 (TIME_INTEGRATION= 2), 1 explicit Euler (TIME_INTEGRATION= 0) */
+	int smoothing;                  /* RESIDUAL_SMOOTHING= */
 } orc_flow;
 
 typedef struct {                    /* each array holds n_cells + (n_faces - n_faces_int) values */
@@ -66,11 +68,13 @@ typedef struct {
 
 typedef struct {
 	int iterations;                 /* EulerSolver::_nbInteration at exit */
-	int converged;                  /* 1 RMS below MIN_RESIDUAL, 2 coefficients stagnated, 0 max_iter */
+	int converged;                  /* 1 RMS below MIN_RESIDUAL, 2 coefficients stagnated, 0 max_iter,
+	                                   3 residual smoothing met a NaN (where the reference exits the process) */
 	int n_rms;                      /* entries written to rms_history */
 	double last_rms;
 	double cl, cd, cm;
 	double force[3], moment[3];
+	long long smooth_sweeps;        /* Jacobi sweeps of residual smoothing, summed over the run */
 } orc_run_stats;
 
 /* FlowField::Initialize (src/solver/FlowField.cpp:68-101) */
@@ -90,8 +94,21 @@ void orc_roe(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, d
  * not pinned to the reference; computeResidual uses it in place of Roe when fl->scheme == 1. */
 void orc_ausm(const orc_mesh *m, const orc_flow *fl, const orc_state *s, int f, double F[5]);
 /* EulerSolver::RungeKutta (src/solver/EulerSolver.cpp:425-472): R holds the residual of the current
- * state on entry and the stage-5 residual on return; dt is scratch [n_cells]. */
-void orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *R, double *dt);
+ * state on entry (smoothed when fl->smoothing) and the stage-5 residual on return; dt is scratch
+ * [n_cells].  Stages 2-5 smooth their residual when fl->smoothing (:456-458).  Returns the Jacobi
+ * sweeps of that smoothing, or -1 if it met a NaN. */
+long long orc_runge_kutta(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *R, double *dt);
+/* EulerSolver::smoothResiduals (src/solver/EulerSolver.cpp:483-518): Jacobi passes
+ * R_c = (R0_c + 0.25 sum_{interior neighbours j} R_j) / (1 + 0.25 n_faces(c)), neighbours in
+ * element2element (= element2face) order.  As the reference's loop behaves: one pass if its
+ * largest change is <= 1e-16, else two.  Returns the number of passes, or -1 if a change of the
+ * first pass is NaN (the reference then exits the process). */
+long long orc_smooth_residuals(const orc_mesh *m, double *R);
+/* EulerSolver::EulerExplicit (src/solver/EulerSolver.cpp:419-423): TimeStepMethod2, ExplicitEuler
+ * (src/solver/TimeIntegration.cpp:78-91) and FlowField::Update (src/solver/FlowField.cpp:103-138).
+ * W [5*n_cells] is the conservative state FlowField keeps (_rho, _rhou, _rhov, _rhow, _rhoE), updated
+ * in place; dt is scratch [n_cells]. */
+void orc_euler_explicit(const orc_mesh *m, const orc_flow *fl, orc_state *s, double *W, const double *R, double *dt);
 /* EulerSolver::computeRMS (src/solver/EulerSolver.cpp:382-389) followed by the sqrt of :99 */
 double orc_rms(const orc_mesh *m, const double *R);
 /* AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52) */

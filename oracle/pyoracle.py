@@ -42,7 +42,8 @@ class OrcFlow(C.Structure):
                 ("w_inf", C.c_double), ("E_inf", C.c_double), ("H_inf", C.c_double), ("M_inf", C.c_double),
                 ("sref", C.c_double), ("cref", C.c_double), ("ref_point", C.c_double * 3),
                 ("cl_axis", C.c_int), ("cl_sign", C.c_int), ("cd_axis", C.c_int), ("cd_sign", C.c_int),
-                ("cm_axis", C.c_int), ("cm_sign", C.c_int), ("scheme", C.c_int)]
+                ("cm_axis", C.c_int), ("cm_sign", C.c_int), ("scheme", C.c_int), ("integrator", C.c_int),
+                ("smoothing", C.c_int)]
 
 
 class OrcState(C.Structure):
@@ -57,7 +58,7 @@ class OrcRunParams(C.Structure):
 class OrcRunStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("n_rms", C.c_int), ("last_rms", C.c_double),
                 ("cl", C.c_double), ("cd", C.c_double), ("cm", C.c_double), ("force", C.c_double * 3),
-                ("moment", C.c_double * 3)]
+                ("moment", C.c_double * 3), ("smooth_sweeps", C.c_longlong)]
 
 
 _lib = None
@@ -78,6 +79,10 @@ def lib() -> C.CDLL:
         L.orc_roe.argtypes = [M, F, S, C.c_int, _dp]
         L.orc_ausm.argtypes = [M, F, S, C.c_int, _dp]
         L.orc_runge_kutta.argtypes = [M, F, S, _dp, _dp]
+        L.orc_runge_kutta.restype = C.c_longlong
+        L.orc_smooth_residuals.argtypes = [M, _dp]
+        L.orc_smooth_residuals.restype = C.c_longlong
+        L.orc_euler_explicit.argtypes = [M, F, S, _dp, _dp, _dp]
         L.orc_rms.argtypes = [M, _dp]
         L.orc_rms.restype = C.c_double
         L.orc_aero_coefficients.argtypes = [M, F, S, _dp, _dp]
@@ -133,9 +138,12 @@ class Mesh:
 
 
 def flow(mach: float, aoa: float = 0.0, gamma: float = 1.4, cfl: float = 1.5, sref: float = 1.0,
-         cref: float = 1.0, ref_point=(0.25, 0.0, 0.0), cl=(1, 1), cd=(0, 1), cm=(2, 1), scheme: int = 0) -> OrcFlow:
+         cref: float = 1.0, ref_point=(0.25, 0.0, 0.0), cl=(1, 1), cd=(0, 1), cm=(2, 1), scheme: int = 0,
+         integrator: int = 0, smoothing: bool = False) -> OrcFlow:
+    """Flow settings; ``integrator`` 0 is RK5 (TIME_INTEGRATION= 2), 1 explicit Euler (TIME_INTEGRATION= 0)."""
     f = OrcFlow()
     f.scheme = scheme
+    f.integrator, f.smoothing = integrator, int(bool(smoothing))
     f.gamma, f.cfl, f.mach, f.aoa_deg = gamma, cfl, mach, aoa
     f.sref, f.cref = sref, cref
     f.ref_point[:] = list(ref_point)
@@ -186,6 +194,13 @@ def runge_kutta(mesh: Mesh, fl: OrcFlow, s: State, R: np.ndarray) -> np.ndarray:
     dt = np.zeros(mesh.n_cells)
     lib().orc_runge_kutta(C.byref(mesh.c), C.byref(fl), C.byref(s.c), _d(R), _d(dt))
     return R.reshape(-1, 5)
+
+
+def smooth_residuals(mesh: Mesh, R: np.ndarray):
+    """EulerSolver::smoothResiduals on a copy of R; returns (smoothed R [n, 5], sweeps or -1)."""
+    R = np.ascontiguousarray(R, dtype=np.float64).reshape(-1).copy()
+    n = lib().orc_smooth_residuals(C.byref(mesh.c), _d(R))
+    return R.reshape(-1, 5), int(n)
 
 
 def rms(mesh: Mesh, R: np.ndarray) -> float:

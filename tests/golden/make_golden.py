@@ -10,7 +10,11 @@ For each small seeded case it stores, as one compressed .npz:
 * ``n_hist`` iterations of Run() from the freestream (``e3d_ref_driver history``): the density RMS
   of every iteration and the final state.
 
-Run from the repository root:  python tests/golden/make_golden.py
+``integrators.npz`` holds Run() histories of three cases under the other time-integration settings
+(TIME_INTEGRATION= 0 explicit Euler, with and without RESIDUAL_SMOOTHING= 1, and RK5 with residual
+smoothing): the density RMS of every iteration and the final state.
+
+Run from the repository root:  python tests/golden/make_golden.py [integrators]
 """
 import os
 import shutil
@@ -30,13 +34,17 @@ from cases import CASES, perturbed_state  # noqa: E402
 from euler3d_b200 import meshgen as mg  # noqa: E402
 
 GOLDEN_CASES = {"channel": 40, "channel_supersonic": 30, "ogrid": 30, "tets": 30}
+# (TIME_INTEGRATION=, RESIDUAL_SMOOTHING=, iterations) per variant, for these cases
+INTEGRATOR_VARIANTS = {"euler": (0, 0, 30), "euler_smooth": (0, 1, 20), "rk5_smooth": (2, 1, 10)}
+INTEGRATOR_CASES = ("channel", "ogrid", "tets")
 REFERENCE_TEST_MESHES = ("StructuredBlock_8.su2", "naca0012_9x9x5_unittest_mesh.su2", "stackedCubes.su2",
                          "stackedTetrahedron.su2")
 
 
-def case_config(case):
+def case_config(case, time_integration=2, residual_smoothing=0):
     return mg.CaseConfig(mach=case.mach, aoa=case.aoa, cfl=case.cfl, max_iter=1, sampling=1,
-                         orientation_cl=2, orientation_cd=0, ref_point=(0.25, 0.0, 0.0))
+                         orientation_cl=2, orientation_cd=0, ref_point=(0.25, 0.0, 0.0),
+                         time_integration=time_integration, residual_smoothing=residual_smoothing)
 
 
 def write_state(path, st):
@@ -85,6 +93,23 @@ def make_case(name, n_hist, work):
     return sum(v.nbytes for v in out.values())
 
 
+def make_integrators(work):
+    out = {}
+    for name in INTEGRATOR_CASES:
+        case = CASES[name]
+        raw = case.raw()
+        for var, (ti, rs, n) in INTEGRATOR_VARIANTS.items():
+            d = os.path.join(work, f"{name}_{var}")
+            cfg = mg.write_case(raw, case_config(case, ti, rs), d)
+            po.ref_call("history", cfg, os.path.join(d, "hist"), str(n))
+            hd = os.path.join(d, "hist")
+            out[f"{name}__{var}__rms"] = np.fromfile(os.path.join(hd, "rms.f64"))
+            for k in po.STATE_KEYS:
+                out[f"{name}__{var}__final_{k}"] = np.fromfile(os.path.join(hd, f"{k}.f64"))
+    np.savez_compressed(os.path.join(HERE, "integrators.npz"), **out)
+    return sum(v.nbytes for v in out.values())
+
+
 def make_reference_meshes(work, reference_root):
     out = {}
     for f in REFERENCE_TEST_MESHES:
@@ -109,6 +134,10 @@ def main():
         sys.exit("reference checker binary missing: run `make -C oracle ref` first")
     work = tempfile.mkdtemp(prefix="e3dgold")
     try:
+        if sys.argv[1:] == ["integrators"]:
+            print("integrators", make_integrators(work), "bytes")
+            return
+        print("integrators", make_integrators(work), "bytes")
         for name, n in GOLDEN_CASES.items():
             print(name, make_case(name, n, work), "bytes")
         ref_root = os.environ.get("E3D_REFERENCE_ROOT", "/root/reference")

@@ -115,3 +115,55 @@ def test_live_against_reference_binary(seed, tmp_path):
         for k in po.STATE_KEYS:
             assert_bitwise(s.a[k], ref_rk[k], f"state after RungeKutta ({k})")
         shutil.rmtree(d, ignore_errors=True)
+
+
+INTEGRATORS = os.path.join(GOLDEN, "integrators.npz")
+# variant -> (integrator (0 RK5, 1 explicit Euler), residual smoothing)
+INTEGRATOR_VARIANTS = {"euler": (1, False), "euler_smooth": (1, True), "rk5_smooth": (0, True)}
+
+
+@pytest.mark.parametrize("name", ["channel", "ogrid", "tets"])
+@pytest.mark.parametrize("variant", list(INTEGRATOR_VARIANTS))
+def test_integrators_match_reference(name, variant):
+    """Explicit Euler (TIME_INTEGRATION= 0) and residual smoothing (RESIDUAL_SMOOTHING= 1), with RK5
+    too: the oracle's Run() history and final state equal the reference's bit for bit."""
+    g = np.load(INTEGRATORS)
+    z, m, _ = load(name)
+    mach, aoa, cfl, gamma = z["flow"]
+    integ, smooth = INTEGRATOR_VARIANTS[variant]
+    fl = po.flow(mach, aoa, gamma, cfl, integrator=integ, smoothing=smooth)
+    ref_rms = g[f"{name}__{variant}__rms"]
+    s = po.freestream(m, fl)
+    st, hist = po.run(m, fl, s, len(ref_rms))
+    assert st.iterations == len(ref_rms)
+    assert (st.smooth_sweeps > 0) == smooth
+    assert_bitwise(hist, ref_rms, "density RMS history")
+    for k in po.STATE_KEYS:
+        assert_bitwise(s.a[k], g[f"{name}__{variant}__final_{k}"], f"final state ({k})")
+
+
+def test_smoothing_passes():
+    """One Jacobi pass when nothing changes by more than 1e-16, else exactly two (the reference's
+    loop ends after its second pass); each pass is R_c = (R0_c + 0.25 sum R_j) / (1 + 0.25 n)."""
+    z, m, _ = load("tets")
+    R0 = np.random.default_rng(0).standard_normal((m.n_cells, 5))
+    Rs, n = po.smooth_residuals(m, R0)
+    assert n == 2
+    f2c = np.asarray(m.a["face2cell"]).reshape(-1, 2)
+    c2f_ptr, c2f = np.asarray(m.a["cell2face_ptr"]), np.asarray(m.a["cell2face"])
+
+    def jacobi(last):
+        out = np.empty_like(last)
+        for c in range(m.n_cells):
+            faces = c2f[c2f_ptr[c]:c2f_ptr[c + 1]]
+            nb = [f2c[f][1] if f2c[f][0] == c else f2c[f][0] for f in faces]
+            s = np.zeros(5)
+            for j in nb:
+                if j < m.n_cells:
+                    s = s + last[j] * 0.25
+            out[c] = (R0[c] + s) / (1 + len(faces) * 0.25)
+        return out
+
+    assert np.array_equal(Rs, jacobi(jacobi(R0)))
+    Z, n0 = po.smooth_residuals(m, np.zeros((m.n_cells, 5)))
+    assert n0 == 1 and not Z.any()
