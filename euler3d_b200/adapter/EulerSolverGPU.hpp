@@ -139,19 +139,27 @@ public:
             _flow.setH((int)i, st[6][i]);
             _flow.setM((int)i, st[7][i]);
         }
-        // residuals.dat: every SAMPLING-th iteration as the reference writes it (src/solver/EulerSolver.cpp:253-259)
         std::vector<double> hist(_stats.n_rms);
         int32_t cnt = 0;
         check(e3d_solver_rms_history(_solver, hist.data(), (int32_t)hist.size(), &cnt), "e3d_solver_rms_history");
         _rms = hist;
+        // residuals.dat, which the reference writes row by row during Run() (ResidualsFile,
+        // include/solver/ResidualsFile.hpp:18-48): the same rows, written once the run is over
+        if (_mpi.getRankID() == 0)
+            check(e3d_solver_write_residuals(_solver, (_config.GetoutputDir() / "residuals.dat").c_str()),
+                  "e3d_solver_write_residuals");
     }
 
-    // The reference's summary (src/solver/EulerSolver.cpp:169-198) without the toml dependency.
+    // EulerSolver::WriteSummary (src/solver/EulerSolver.cpp:169-198): cp_part_N.dat and summary.txt,
+    // byte for byte as the reference writes them.  The .sol/.bry files come from the reference's own
+    // WriteSolution on the FlowField that Run() filled.
     void WriteSummary(long solverTimer, long totalTimer) {
-        std::ofstream f(_config.GetoutputDir() / "summary.txt");
-        f << "Iterations = " << _stats.iterations << "\nSolverLoopTime_ms = " << solverTimer
-          << "\nTotalSolverTime_ms = " << totalTimer << "\nCL = " << _stats.cl << "\nCD = " << _stats.cd
-          << "\nCM = " << _stats.cm << "\nNElem = " << _mesh.GetNElemGlobalMesh() << "\n";
+        const std::string cp = "cp_part_" + std::to_string(_mpi.getRankID()) + ".dat";
+        check(e3d_solver_write_cp(_solver, (_config.GetoutputDir() / cp).c_str()), "e3d_solver_write_cp");
+        if (_mpi.getRankID() == 0)
+            check(e3d_solver_write_summary(_solver, (_config.GetoutputDir() / "summary.txt").c_str(), solverTimer,
+                                           totalTimer, _mpi.getPoolSize()),
+                  "e3d_solver_write_summary");
     }
 
     const e3d_run_stats &stats() const { return _stats; }

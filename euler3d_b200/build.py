@@ -30,6 +30,7 @@ SOURCES = [
     ("stage_f32.cu", ["-fmad=true"]),
     ("solver.cu", ["-fmad=false"]),
     ("batch.cu", ["-fmad=false"]),
+    ("outputs.cu", ["-fmad=false"]),
     ("capi.cpp", []),
     ("mesh_prep.cpp", []),
 ]

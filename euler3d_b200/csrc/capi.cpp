@@ -1,4 +1,5 @@
 // Mesh half of the C ABI (include/euler3d_b200.h) plus status strings and error reporting.
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -164,6 +165,24 @@ e3d_status e3d_mesh_array(const e3d_mesh *mesh, const char *name, const void **d
         }
     set_last_error(std::string("unknown mesh array '") + name + "'");
     return E3D_ERR_INVALID_ARG;
+}
+
+e3d_status e3d_mesh_write_boundary(const e3d_mesh *mesh, const char *path) {
+    return guarded([&] {
+        if (!mesh || !path) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        const PreparedMesh &m = mesh->m;
+        FILE *f = std::fopen(path, "w");
+        if (!f) throw Error(E3D_ERR_INVALID_ARG, std::string("cannot open ") + path + " for writing");
+        std::fprintf(f, "NOMBRE DE CELLULES= %zu\n", m.wall_ghost.size());
+        for (size_t i = 0; i < m.wall_ghost.size(); i++) {
+            const int face = m.wall_face[i];
+            const int a = m.face2node_ptr[face], b = m.face2node_ptr[face + 1];
+            std::fprintf(f, "%9d%9d", m.wall_interior[i], b - a);
+            for (int k = a; k < b; k++) std::fprintf(f, "%9d", m.face2node[k]);
+            std::fprintf(f, "\n");
+        }
+        if (std::fclose(f) != 0) throw Error(E3D_ERR_INVALID_ARG, "writing the boundary file failed");
+    });
 }
 
 e3d_status e3d_mesh_describe(const e3d_mesh *mesh, e3d_mesh_desc *d) {

@@ -101,6 +101,7 @@ __device__ __forceinline__ void coeff_body(const CoeffArgs &a, double (*terms)[k
             if (i < a.n_wall) {
                 double p = wall_pressure(a, a.cell[i]);
                 double cp = a.cp_factor * (p - a.p_inf);
+                if (a.cp_out) a.cp_out[i] = cp;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
                     double coeff = a.svec[3 * i + k] * cp * a.cref / a.sref;
@@ -144,6 +145,7 @@ __device__ __forceinline__ void coeff_body(const CoeffArgs &a, double (*terms)[k
             for (int u = 0; u < U; u++) {
                 if (base + u * kCoeffThreads >= a.n_wall) break;
                 const double cp = a.cp_factor * (p[u] - a.p_inf);
+                if (a.cp_out) a.cp_out[base + u * kCoeffThreads] = cp;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
                     const double coeff = sv[u][k] * cp * a.cref / a.sref;
@@ -181,6 +183,15 @@ __device__ __forceinline__ void coeff_body(const CoeffArgs &a, double (*terms)[k
     double tol = ctl->min_aero;
     bool ok = fabs(ctl->cl - cl) < tol && fabs(ctl->cd - cd) < tol && fabs(ctl->cm - cm) < tol;
     ctl->counter = ok ? ctl->counter + 1 : 0;
+    if (a.samples && ctl->n_samples < ctl->sample_cap) {  // a residuals.dat row (EulerSolver::PrintInfo)
+        double *s = a.samples + 7 * (size_t)ctl->n_samples;
+        s[0] = ctl->it;
+        for (int k = 0; k < 3; k++) {
+            s[1 + k] = F[k];
+            s[4 + k] = M[k];
+        }
+    }
+    ctl->n_samples += 1;
     ctl->cl = cl;
     ctl->cd = cd;
     ctl->cm = cm;
@@ -833,6 +844,12 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     S->wall_cell.upload(wcell, s);
     S->wall_svec.upload(wsv, s);
     S->wall_center.upload(wct, s);
+    S->wall_cp.alloc(std::max(d->n_wall, 1));
+    E3D_CUDA(cudaMemsetAsync(S->wall_cp.p, 0, S->wall_cp.n * sizeof(double), s));
+    // AeroCoefficients' sum of the wall face vectors (src/solver/AeroCoefficients.cpp:29-33)
+    for (int i = 0; i < d->n_wall; i++)
+        for (int k = 0; k < 3; k++) S->wall_sum[k] += wsv[3 * i + k];
+    S->wall_center_host = wct;
     S->f32 = p->precision == E3D_PREC_FP32_FLUX;
     if (S->f32) {
         if (!S->tiles_ok) throw Error(E3D_ERR_INVALID_ARG, "FP32_FLUX mode needs face tiles this mesh cannot form");
@@ -941,7 +958,8 @@ static Solver *solo(e3d_solver *s) {
 // A fresh control block for a run -- a new EulerSolver's counters (_nbInteration = 0,
 // _CL = _CD = _CM = 0, src/solver/EulerSolver.cpp:21-58) -- keeping whether the loaded interior
 // Mach still holds.  Reads the old block back first (synchronises stream s once).
-static void init_control(Solver *S, const e3d_run_params *rp, int max_iter, int hist_cap, cudaStream_t s) {
+static void init_control(Solver *S, const e3d_run_params *rp, int max_iter, int hist_cap, int sample_cap,
+                         cudaStream_t s) {
     E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
     E3D_CUDA(cudaStreamSynchronize(s));
     Control init{};
@@ -952,6 +970,7 @@ static void init_control(Solver *S, const e3d_run_params *rp, int max_iter, int 
     init.min_res = rp->min_residual;
     init.min_aero = rp->min_aerocoeff_error;
     init.min_drop = rp->min_residual_drop;
+    init.sample_cap = sample_cap;
     init.done = max_iter == 0;
     std::memcpy(S->ctl_host, &init, sizeof init);
     E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, s));
@@ -983,7 +1002,21 @@ void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s) {
             S->graph = nullptr;
         }
     }
-    init_control(S, rp, max_iter, S->hist_cap, s);
+    // one sample every `sampling` iterations: max_iter / sampling rows at most
+    const int need = max_iter / rp->sampling + 1;
+    if (S->sample_cap < need || !S->samples.p) {
+        E3D_CUDA(cudaStreamSynchronize(s));
+        S->samples.release();
+        S->samples.alloc(7 * (size_t)need);
+        S->sample_cap = need;
+        if (S->graph) {  // the captured coefficient kernels hold the old pointer
+            cudaGraphExecDestroy(S->graph);
+            S->graph = nullptr;
+        }
+    }
+    // a fresh AeroCoefficients: Cp of every wall face zero until the first sample
+    if (S->n_wall) E3D_CUDA(cudaMemsetAsync(S->wall_cp.p, 0, S->n_wall * sizeof(double), s));
+    init_control(S, rp, max_iter, S->hist_cap, S->sample_cap, s);
     state_to_buffer0(S, s);
 }
 
@@ -1280,7 +1313,7 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
         // the history region starts cleared, so no entry of an earlier call can be read back
         E3D_CUDA(cudaMemsetAsync(hist, 0, (size_t)std::max(max_iter, 1) * sizeof(double), S->stream));
         if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
-        init_control(S, rp, max_iter, kNoAllocMaxIter, S->stream);
+        init_control(S, rp, max_iter, kNoAllocMaxIter, 0, S->stream);
         state_to_buffer0(S, S->stream);
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
         const int every = rp->check_every > 0 ? rp->check_every : 32;

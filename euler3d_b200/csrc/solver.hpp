@@ -48,6 +48,8 @@ struct CoeffArgs {
     int run_mode;                       // 1: sampled inside e3d_solver_run, apply the stop test
     int sequential;                     // 1: sum in the reference's wall order (FP64_EXACT)
     double *__restrict__ out;           // 6 doubles (force, moment) when not in run mode
+    double *__restrict__ cp_out;        // [n_wall] Cp of every wall face (AeroCoefficients::_cp), or null
+    double *__restrict__ samples;       // run mode: 7 doubles (iteration, force, moment) per sample, or null
 };
 
 // Arguments of the RMS / stop-test kernel of one solver.
@@ -139,6 +141,12 @@ struct Solver {
     // residual smoothing: interior neighbours (element2face order), denominators, residual arrays
     // r0 (the stage's residual), r1, r2 (after the first / second Jacobi pass), pass flags
     bool smoothing = false;
+    // output files: the last run's coefficient samples, the wall Cp of the last sample, and host
+    // copies of the wall geometry (reference wall order)
+    DevBuf<double> samples, wall_cp;
+    int sample_cap = 0;
+    double wall_sum[3] = {0, 0, 0};
+    std::vector<double> wall_center_host;
     DevBuf<int> nb_ptr, nb;
     DevBuf<double> den, rbuf;
     DevBuf<unsigned long long> smooth_flags;
@@ -178,6 +186,8 @@ struct Solver {
                                 &scratch, &den, &rbuf};
         nb_ptr.release();
         nb.release();
+        samples.release();
+        wall_cp.release();
         smooth_flags.release();
         for (auto *b : db) b->release();
         if (ctl) cudaFree(ctl);
@@ -194,7 +204,7 @@ struct Solver {
                (int64_t)tile_rec32_off.n * 8 +
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
-                         hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n) * 8 +
+                         hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n + samples.n + wall_cp.n) * 8 +
                (int64_t)(nb_ptr.n + nb.n) * 4 + (int64_t)sizeof(Control);
     }
 
@@ -348,6 +358,8 @@ struct Solver {
         c.w0_stride = w0_stride;
         c.gamma = prm.gamma;
         c.out = out;
+        c.cp_out = wall_cp.p;
+        c.samples = run_mode ? samples.p : nullptr;
         return c;
     }
 

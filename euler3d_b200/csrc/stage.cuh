@@ -49,6 +49,8 @@ struct Control {
     double min_res, min_aero, last_rms, cl, cd, cm;
     double min_drop;   // > 0: also stop once the RMS is below min_drop x the run's first RMS
     double rms0;       // RMS of the run's first iteration
+    int n_samples;     // coefficient samples taken (residuals.dat rows)
+    int sample_cap;    // capacity of the sample record
     double force[3], moment[3];
 };
 

@@ -34,6 +34,10 @@ def _ip(a: np.ndarray):
 class Mesh:
     """A mesh prepared by the library: connectivity, metrics and ghost lists in the reference numbering."""
 
+    def write_boundary(self, path: str) -> None:
+        """``<partition>.bry`` as the reference's WriteSolution writes it (wall cells and face nodes)."""
+        check(_lib.load().e3d_mesh_write_boundary(self._h, path.encode()))
+
     def __init__(self, handle: C.c_void_p):
         self._h = handle
 
@@ -288,3 +292,33 @@ class EulerSolver:
         f, m = np.empty(3), np.empty(3)
         check(_lib.load().e3d_solver_coefficients(self._h, _dp(f), _dp(m)))
         return f, m
+
+    # ---- the reference's output files (byte for byte)
+    def coefficient_history(self) -> np.ndarray:
+        """[n, 7]: iteration, force (3), moment (3) of every sample of the last run."""
+        n = C.c_int32()
+        check(_lib.load().e3d_solver_coefficient_history(self._h, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 7))
+        check(_lib.load().e3d_solver_coefficient_history(self._h, _dp(out), n.value, C.byref(n)))
+        return out[: n.value]
+
+    def wall_cp(self) -> np.ndarray:
+        n = C.c_int32()
+        check(_lib.load().e3d_solver_wall_cp(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1))
+        check(_lib.load().e3d_solver_wall_cp(self._h, _dp(out), n.value, C.byref(n)))
+        return out[: n.value]
+
+    def write_outputs(self, output_dir: str, partition_file: Optional[str] = None, solver_ms: int = 0,
+                      total_ms: int = 0, n_cores: int = 1, rank: int = 0) -> None:
+        """residuals.dat, cp_part_<rank>.dat and summary.txt into ``output_dir`` and, given the
+        partition file name, ``<partition_file>.sol`` (src/Solver.cpp:58-67 writes the same set)."""
+        import os
+
+        lib = _lib.load()
+        check(lib.e3d_solver_write_residuals(self._h, os.path.join(output_dir, "residuals.dat").encode()))
+        check(lib.e3d_solver_write_summary(self._h, os.path.join(output_dir, "summary.txt").encode(), solver_ms,
+                                           total_ms, n_cores))
+        check(lib.e3d_solver_write_cp(self._h, os.path.join(output_dir, f"cp_part_{rank}.dat").encode()))
+        if partition_file:
+            check(lib.e3d_solver_write_solution(self._h, (partition_file + ".sol").encode()))

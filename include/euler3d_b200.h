@@ -128,6 +128,10 @@ typedef struct e3d_mesh_desc {
 	const int32_t *sym_ghost, *sym_interior, *sym_face;
 } e3d_mesh_desc;
 
+/* <partition>.bry, WriteSolution::writeBoundaryFile (src/solver/WriteSolution.cpp:57-76): every wall
+ * face's interior cell and node ids, byte for byte as the reference writes it. */
+e3d_status e3d_mesh_write_boundary(const e3d_mesh *mesh, const char *path);
+
 /* Fill a descriptor whose pointers refer to a prepared mesh's arrays. */
 e3d_status e3d_mesh_describe(const e3d_mesh *mesh, e3d_mesh_desc *desc);
 
@@ -246,6 +250,28 @@ e3d_status e3d_solver_residual(e3d_solver *solver, double *residual, double *dt)
 
 /* AeroCoefficients::Update (src/solver/AeroCoefficients.cpp:38-52) on the current state. */
 e3d_status e3d_solver_coefficients(e3d_solver *solver, double force[3], double moment[3]);
+
+/* The coefficient samples of the last run: 7 doubles each -- the iteration, the force and the moment
+ * coefficient vectors -- one per SAMPLING-th iteration (the rows EulerSolver::PrintInfo writes to
+ * residuals.dat, src/solver/EulerSolver.cpp:253-259).  *count receives the number of samples. */
+e3d_status e3d_solver_coefficient_history(e3d_solver *solver, double *samples, int32_t capacity, int32_t *count);
+/* Pressure coefficient of every wall face (reference wall order) at the last sample of the last run
+ * (AeroCoefficients::_cp; zero before the first sample) or of the last e3d_solver_coefficients. */
+e3d_status e3d_solver_wall_cp(e3d_solver *solver, double *cp, int32_t capacity, int32_t *count);
+
+/* The reference's output files of the last run, byte for byte as the reference writes them:
+ *   residuals.dat   ResidualsFile (include/solver/ResidualsFile.hpp:18-48): one row per sample, plus
+ *                   the row the residual exit prints (src/solver/EulerSolver.cpp:100-108)
+ *   cp_part_N.dat   EulerSolver::PrintCp (:283-303): wall Cp of the last sample and face centroids
+ *   <partition>.sol WriteSolution::writeSolutionFile (src/solver/WriteSolution.cpp:30-55): the
+ *                   interior cells' density, velocity, pressure and energy
+ *   summary.txt     EulerSolver::WriteSummary (:169-198), the TOML the reference's toml++ prints,
+ *                   with the caller's timings (milliseconds) and core count */
+e3d_status e3d_solver_write_residuals(e3d_solver *solver, const char *path);
+e3d_status e3d_solver_write_cp(e3d_solver *solver, const char *path);
+e3d_status e3d_solver_write_solution(e3d_solver *solver, const char *path);
+e3d_status e3d_solver_write_summary(e3d_solver *solver, const char *path, int64_t solver_ms, int64_t total_ms,
+                                    int32_t n_cores);
 
 /* ------------------------------------------------------------------------------------------
  * Batches: many solvers advanced together.  No counterpart in the reference, whose solver runs one

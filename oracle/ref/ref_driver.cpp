@@ -18,6 +18,8 @@
  *                                  computeResidual, updateDeltaTime, RungeKutta)
  *                                  from the freestream or a given state
  *   bench   <cfg> <warm> <iters>   time Run() over <iters> iterations
+ *   outputs <cfg> <out> <solver_ms> <total_ms>   Run(), WriteSummary and WriteSolution: the
+ *                                  reference's own output files
  *
  * Private members are reached through the access-specifier macro below only
  * to READ the solver's residual / time-step vectors, to reset its iteration
@@ -56,6 +58,7 @@
 #include "parser/SimConfig.hpp"
 #include "solver/EulerSolver.hpp"
 #include "solver/FlowField.hpp"
+#include "solver/WriteSolution.hpp"
 #undef private
 #undef protected
 
@@ -224,6 +227,17 @@ int main(int argc, char **argv) {
 		     << fmt17(solver._momentCoefficients.x) << " " << fmt17(solver._momentCoefficients.y) << " "
 		     << fmt17(solver._momentCoefficients.z) << "\n";
 		writeText("meta.txt", meta.str());
+		return 0;
+	}
+
+	if (mode == "outputs") {
+		// the files a run writes (src/Solver.cpp:58-67): residuals.dat during Run(), then
+		// WriteSummary (summary.txt, cp_part_0.dat) with the given timings, then WriteSolution
+		// (<partition>.sol, <partition>.bry)
+		if (argc < 6) return 2;
+		solver.Run();
+		solver.WriteSummary(std::atol(argv[4]), std::atol(argv[5]));
+		Solver::WriteSolution ws(flow, localmesh, config, e3d_mpi);
 		return 0;
 	}
 

@@ -14,7 +14,11 @@ For each small seeded case it stores, as one compressed .npz:
 (TIME_INTEGRATION= 0 explicit Euler, with and without RESIDUAL_SMOOTHING= 1, and RK5 with residual
 smoothing): the density RMS of every iteration and the final state.
 
-Run from the repository root:  python tests/golden/make_golden.py [integrators]
+``outputs/<run>/`` holds the files the reference's own writers produce for two short runs of the
+bump channel (``e3d_ref_driver outputs``, timings fixed at 1234 / 5678 ms): residuals.dat,
+cp_part_0.dat, summary.txt, mesh.par.sol and mesh.par.bry, with the run's settings in run.json.
+
+Run from the repository root:  python tests/golden/make_golden.py [integrators | outputs]
 """
 import os
 import shutil
@@ -110,6 +114,37 @@ def make_integrators(work):
     return sum(v.nbytes for v in out.values())
 
 
+# run name -> (case, TIME_INTEGRATION=, MAX_ITER=, SAMPLING=, MIN_RESIDUAL as a fraction of the first RMS)
+OUTPUT_RUNS = {"rk5_max_iter": ("channel", 2, 25, 4, 0.0), "euler_residual_exit": ("channel", 0, 400, 7, 1e-2)}
+
+
+def make_outputs(work):
+    import json
+
+    for run, (name, ti, max_iter, sampling, drop) in OUTPUT_RUNS.items():
+        case = CASES[name]
+        min_res = 0.0
+        if drop:  # the absolute MIN_RESIDUAL: a fraction of the first iteration's RMS
+            d0 = os.path.join(work, run + "_first")
+            cfg0 = mg.write_case(case.raw(), case_config(case, ti), d0)
+            po.ref_call("history", cfg0, os.path.join(d0, "hist"), "1")
+            min_res = float(np.fromfile(os.path.join(d0, "hist", "rms.f64"))[0]) * drop
+        d = os.path.join(work, run)
+        cfg = mg.CaseConfig(mach=case.mach, aoa=case.aoa, cfl=case.cfl, max_iter=max_iter, sampling=sampling,
+                            min_residual=min_res, orientation_cl=2, orientation_cd=0, ref_point=(0.25, 0.0, 0.0),
+                            time_integration=ti)
+        cfg_path = mg.write_case(case.raw(), cfg, d)
+        po.ref_call("outputs", cfg_path, os.path.join(d, "o"), "1234", "5678")
+        dst = os.path.join(HERE, "outputs", run)
+        os.makedirs(dst, exist_ok=True)
+        for src in ("output/residuals.dat", "output/cp_part_0.dat", "output/summary.txt", "mesh.par.sol",
+                    "mesh.par.bry"):
+            shutil.copy(os.path.join(d, src), os.path.join(dst, os.path.basename(src)))
+        with open(os.path.join(dst, "run.json"), "w") as f:
+            json.dump({"case": name, "time_integration": ti, "max_iter": max_iter, "sampling": sampling,
+                       "min_residual": min_res, "solver_ms": 1234, "total_ms": 5678}, f, indent=1)
+
+
 def make_reference_meshes(work, reference_root):
     out = {}
     for f in REFERENCE_TEST_MESHES:
@@ -137,6 +172,10 @@ def main():
         if sys.argv[1:] == ["integrators"]:
             print("integrators", make_integrators(work), "bytes")
             return
+        if sys.argv[1:] == ["outputs"]:
+            make_outputs(work)
+            return
+        make_outputs(work)
         print("integrators", make_integrators(work), "bytes")
         for name, n in GOLDEN_CASES.items():
             print(name, make_case(name, n, work), "bytes")
