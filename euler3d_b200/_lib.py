@@ -109,6 +109,8 @@ SIGNATURES = {
     "e3d_solver_write_solution": (C.c_int, [C.c_void_p, C.c_char_p]),
     "e3d_solver_write_summary": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64, C.c_int64, C.c_int32]),
     "e3d_mesh_write_boundary": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "e3d_mesh_read_partitions": (C.c_int, [C.POINTER(C.c_char_p), C.c_int32, C.c_double, C.c_int32,
+                                           C.POINTER(C.c_void_p)]),
     "e3d_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "e3d_batch_destroy": (None, [C.c_void_p]),
     "e3d_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunParams)]),

@@ -62,6 +62,34 @@ e3d_status e3d_mesh_read(const char *path, double cref, int32_t n_threads, e3d_m
     return st;
 }
 
+e3d_status e3d_mesh_read_partitions(const char *const *paths, int32_t n_parts, double cref, int32_t n_threads,
+                                    e3d_mesh **out) {
+    if (!paths || !out || n_parts <= 0) {
+        set_last_error("NULL argument or no partition files");
+        return E3D_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    std::unique_ptr<e3d_mesh> mesh(new (std::nothrow) e3d_mesh());
+    if (!mesh) return E3D_ERR_OOM;
+    e3d_status st = guarded([&] {
+        if (!(cref != 0.0)) throw Error(E3D_ERR_INVALID_ARG, "cref must be non-zero");
+        std::vector<RawMesh> parts(n_parts);
+        std::vector<std::vector<PartitionInterface>> ifc(n_parts);
+        for (int p = 0; p < n_parts; p++) {
+            if (!paths[p]) throw Error(E3D_ERR_INVALID_ARG, "partition path is NULL");
+            read_su2_partition(paths[p], parts[p], ifc[p]);
+        }
+        RawMesh merged;
+        std::vector<int32_t> cell_ptr;
+        merge_partitions(parts, ifc, merged, cell_ptr);
+        parts.clear();
+        prepare_mesh(merged, cref, mesh->m, n_threads);
+        mesh->m.partition_cell_ptr = std::move(cell_ptr);
+    });
+    if (st == E3D_OK) *out = mesh.release();
+    return st;
+}
+
 e3d_status e3d_mesh_from_arrays(int32_t n_nodes, const double *xyz, int32_t n_elems, const int32_t *elem_vtk,
                                 const int32_t *elem_ptr, const int32_t *elem_nodes, int32_t n_markers,
                                 const char *const *marker_tags, const int32_t *marker_ptr, const int32_t *face_ptr,
@@ -141,6 +169,7 @@ e3d_status e3d_mesh_array(const e3d_mesh *mesh, const char *name, const void **d
     const I ints[] = {{"face2cell", &m.face2cell},         {"cell2face_ptr", &m.cell2face_ptr},
                       {"cell2face", &m.cell2face},         {"cell2cell", &m.cell2cell},
                       {"face2node_ptr", &m.face2node_ptr}, {"face2node", &m.face2node},
+                      {"partition_cell_ptr", &m.partition_cell_ptr},
                       {"wall_ghost", &m.wall_ghost},       {"wall_interior", &m.wall_interior},
                       {"wall_face", &m.wall_face},         {"farfield_ghost", &m.farfield_ghost},
                       {"farfield_interior", &m.farfield_interior}, {"farfield_face", &m.farfield_face},

@@ -9,7 +9,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <fstream>
+#include <numeric>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -458,7 +460,7 @@ int surface_nodes(int vtk) {
 
 }  // namespace
 
-void read_su2(const std::string &path, RawMesh &out) {
+static void read_su2_impl(const std::string &path, RawMesh &out, std::vector<PartitionInterface> *interfaces) {
     LineReader r(path);
     if (!r.in) throw std::runtime_error("cannot open mesh file " + path);
     out = RawMesh();
@@ -517,11 +519,149 @@ void read_su2(const std::string &path, RawMesh &out) {
         }
         out.markers.push_back(std::move(mk));
     }
-    // A .par file ends with the inter-partition markers; one domain must have none.
+    // A .par file ends with the inter-partition markers (MeshPartition::parseMpiBoundaryElement)
     while (r.next()) {
         const char *v = value_after(r.line, "NINTERNAL_MARKER=");
-        if (v && std::strtol(v, nullptr, 10) != 0)
-            throw std::runtime_error("partition file " + path + " has inter-partition markers; give the whole mesh");
+        if (!v) continue;
+        const long n_adj = std::strtol(v, nullptr, 10);
+        if (n_adj == 0) break;
+        if (!interfaces)
+            throw std::runtime_error("partition file " + path + " has inter-partition markers; give the whole mesh "
+                                     "or every partition");
+        for (long a = 0; a < n_adj; a++) {
+            PartitionInterface itf;
+            if (!r.next()) throw std::runtime_error("unexpected end of file in NINTERNAL_MARKER section");
+            const char *pv = value_after(r.line, "INTERNAL_MARKER=");
+            if (!pv) throw std::runtime_error("expected INTERNAL_MARKER= in " + path);
+            itf.other = (int32_t)std::strtol(pv, nullptr, 10);
+            if (!r.next()) throw std::runtime_error("unexpected end of file after INTERNAL_MARKER");
+            const char *nv = value_after(r.line, "NELEM_MPI=");
+            if (!nv) throw std::runtime_error("expected NELEM_MPI= in " + path);
+            const long k = std::strtol(nv, nullptr, 10);
+            for (long i = 0; i < k; i++) {
+                if (!r.next()) throw std::runtime_error("unexpected end of file in NELEM_MPI section");
+                char *p = const_cast<char *>(r.line.c_str());
+                itf.this_elem.push_back((int32_t)std::strtol(p, &p, 10));
+                itf.other_elem.push_back((int32_t)std::strtol(p, &p, 10));
+                const int vtk = (int)std::strtol(p, &p, 10);
+                const int n = surface_nodes(vtk);
+                if (n < 0) throw std::runtime_error("unsupported inter-partition face VTK type " + std::to_string(vtk));
+                for (int j = 0; j < n; j++) itf.nodes.push_back((int32_t)std::strtol(p, &p, 10));
+                itf.vtk.push_back(vtk);
+                itf.node_ptr.push_back((int32_t)itf.nodes.size());
+            }
+            interfaces->push_back(std::move(itf));
+        }
+        break;
+    }
+}
+
+void read_su2(const std::string &path, RawMesh &out) { read_su2_impl(path, out, nullptr); }
+
+void read_su2_partition(const std::string &path, RawMesh &out, std::vector<PartitionInterface> &interfaces) {
+    interfaces.clear();
+    read_su2_impl(path, out, &interfaces);
+}
+
+void merge_partitions(const std::vector<RawMesh> &parts, const std::vector<std::vector<PartitionInterface>> &ifc,
+                      RawMesh &out, std::vector<int32_t> &cell_ptr) {
+    const int P = (int)parts.size();
+    if (P == 0 || (int)ifc.size() != P) throw std::runtime_error("no partitions to merge");
+    std::vector<int64_t> noff(P + 1, 0);
+    for (int p = 0; p < P; p++) noff[p + 1] = noff[p] + parts[p].n_nodes();
+    if (noff[P] > INT32_MAX) throw std::runtime_error("too many nodes");
+    // union-find over every partition's local nodes
+    std::vector<int32_t> up(noff[P]);
+    std::iota(up.begin(), up.end(), 0);
+    auto find = [&](int32_t x) {
+        while (up[x] != x) {
+            up[x] = up[up[x]];
+            x = up[x];
+        }
+        return x;
+    };
+    auto bad = [](const std::string &m) { throw std::runtime_error("inconsistent partitions: " + m); };
+    for (int p = 0; p < P; p++) {
+        for (const PartitionInterface &I : ifc[p]) {
+            const int q = I.other;
+            if (q < 0 || q >= P || q == p) bad("neighbour partition " + std::to_string(q) + " out of range");
+            if (q < p) continue;  // each pair once, from its lower partition
+            const PartitionInterface *J = nullptr;
+            for (const PartitionInterface &c : ifc[q])
+                if (c.other == p) J = &c;
+            if (!J) bad("partition " + std::to_string(q) + " lists no faces shared with " + std::to_string(p));
+            if (J->vtk.size() != I.vtk.size())
+                bad("partitions " + std::to_string(p) + " and " + std::to_string(q) + " list different face counts");
+            for (size_t k = 0; k < I.vtk.size(); k++) {
+                if (I.this_elem[k] != J->other_elem[k] || I.other_elem[k] != J->this_elem[k] || I.vtk[k] != J->vtk[k])
+                    bad("face " + std::to_string(k) + " between partitions " + std::to_string(p) + " and " +
+                        std::to_string(q) + " does not match");
+                if (I.this_elem[k] < 0 || I.this_elem[k] >= parts[p].n_elems() || I.other_elem[k] < 0 ||
+                    I.other_elem[k] >= parts[q].n_elems())
+                    bad("inter-partition element id out of range");
+                for (int i = I.node_ptr[k], j = J->node_ptr[k]; i < I.node_ptr[k + 1]; i++, j++) {
+                    const int32_t a = I.nodes[i], b = J->nodes[j];
+                    if (a < 0 || a >= parts[p].n_nodes() || b < 0 || b >= parts[q].n_nodes())
+                        bad("inter-partition node id out of range");
+                    const int32_t ra = find((int32_t)(noff[p] + a)), rb = find((int32_t)(noff[q] + b));
+                    if (ra != rb) up[std::max(ra, rb)] = std::min(ra, rb);
+                }
+            }
+        }
+    }
+    // merged nodes in order of first appearance (partition 0's first); duplicates must agree
+    out = RawMesh();
+    std::vector<int32_t> id(noff[P], -1), merged(noff[P]);
+    for (int p = 0; p < P; p++)
+        for (int32_t i = 0; i < parts[p].n_nodes(); i++) {
+            const int32_t g = (int32_t)(noff[p] + i), r = find(g);
+            if (id[r] < 0) {
+                id[r] = out.n_nodes();
+                for (int k = 0; k < 3; k++) out.xyz.push_back(parts[p].xyz[3 * (size_t)i + k]);
+            } else {
+                for (int k = 0; k < 3; k++)
+                    if (out.xyz[3 * (size_t)id[r] + k] != parts[p].xyz[3 * (size_t)i + k])
+                        bad("a node shared by two partitions has two different coordinates");
+            }
+            merged[g] = id[r];
+        }
+    // elements partition by partition, markers merged by tag (first-appearance order)
+    cell_ptr.assign(1, 0);
+    out.elem_ptr.assign(1, 0);
+    std::vector<std::string> tags;
+    for (int p = 0; p < P; p++) {
+        const RawMesh &m = parts[p];
+        for (int32_t e = 0; e < m.n_elems(); e++) {
+            out.elem_vtk.push_back(m.elem_vtk[e]);
+            for (int32_t k = m.elem_ptr[e]; k < m.elem_ptr[e + 1]; k++) {
+                const int32_t n = m.elem_nodes[k];
+                if (n < 0 || n >= m.n_nodes()) bad("element node id out of range");
+                out.elem_nodes.push_back(merged[noff[p] + n]);
+            }
+            out.elem_ptr.push_back((int32_t)out.elem_nodes.size());
+        }
+        cell_ptr.push_back(out.n_elems());
+        for (const RawMarker &mk : m.markers) {
+            size_t t = 0;
+            while (t < tags.size() && tags[t] != mk.tag) t++;
+            if (t == tags.size()) {
+                tags.push_back(mk.tag);
+                RawMarker nm;
+                nm.tag = mk.tag;
+                nm.node_ptr.push_back(0);
+                out.markers.push_back(std::move(nm));
+            }
+            RawMarker &dst = out.markers[t];
+            for (size_t e = 0; e < mk.vtk.size(); e++) {
+                dst.vtk.push_back(mk.vtk[e]);
+                for (int32_t k = mk.node_ptr[e]; k < mk.node_ptr[e + 1]; k++) {
+                    const int32_t n = mk.nodes[k];
+                    if (n < 0 || n >= m.n_nodes()) bad("marker node id out of range");
+                    dst.nodes.push_back(merged[noff[p] + n]);
+                }
+                dst.node_ptr.push_back((int32_t)dst.nodes.size());
+            }
+        }
     }
 }
 

@@ -46,6 +46,17 @@ struct PreparedMesh {
     std::vector<int32_t> wall_ghost, wall_interior, wall_face;
     std::vector<int32_t> farfield_ghost, farfield_interior, farfield_face;
     std::vector<int32_t> sym_ghost, sym_interior, sym_face;
+    // a mesh merged from partition files: cells of partition p are [ptr[p], ptr[p+1]) (empty otherwise)
+    std::vector<int32_t> partition_cell_ptr;
+};
+
+// The inter-partition faces a .par file lists for one neighbouring partition (NINTERNAL_MARKER=,
+// src/parser/MeshPartition.cpp:39-112, written by src/partition/SU2Writer.cpp:107-124): for each
+// face this partition's element, the neighbour's element (its local id there), the face's VTK type
+// and the face's nodes in this partition's local numbering.
+struct PartitionInterface {
+    int32_t other = -1;
+    std::vector<int32_t> this_elem, other_elem, vtk, node_ptr{0}, nodes;
 };
 
 // Throws std::runtime_error with a message on malformed input.
@@ -55,5 +66,16 @@ void prepare_mesh(const RawMesh &raw, double cref, PreparedMesh &out, int n_thre
 // src/parser/MeshPartition.cpp:39-112).  A .par file's NINTERNAL_MARKER section must be empty
 // (one domain); throws otherwise.
 void read_su2(const std::string &path, RawMesh &out);
+
+// One partition file of a multi-partition case, with its inter-partition faces.
+void read_su2_partition(const std::string &path, RawMesh &out, std::vector<PartitionInterface> &interfaces);
+
+// One mesh from the partitions of a case (the files E3D_PRE writes, src/partition/Partition.cpp):
+// nodes duplicated across partitions are joined through the inter-partition faces both sides list
+// in the same order with the nodes in the same order (src/partition/Partition.cpp:222-296);
+// elements are concatenated partition by partition (cell_ptr[p] = first cell of partition p) and
+// boundary markers merged by tag.  Throws on inconsistent partitions.
+void merge_partitions(const std::vector<RawMesh> &parts, const std::vector<std::vector<PartitionInterface>> &ifc,
+                      RawMesh &out, std::vector<int32_t> &cell_ptr);
 
 }  // namespace e3d

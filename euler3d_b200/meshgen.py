@@ -359,6 +359,95 @@ def write_su2(mesh: RawMesh, path: str, partition: bool = True) -> None:
             f.write("NINTERNAL_MARKER= 0\n")
 
 
+def write_partitions(mesh: RawMesh, n_parts: int, pattern: str) -> List[str]:
+    """Split ``mesh`` into ``n_parts`` slabs along x (cells by the x of their mean node) and write
+    one ``.par`` file per part in the layout of the reference's partitioner (E3D_PRE,
+    src/partition/Partition.cpp:150-296, src/partition/SU2Writer.cpp): each part's elements in
+    ascending global order, its nodes renumbered by first use, its boundary elements, and
+    NINTERNAL_MARKER sections listing every face shared with another part -- the element on each
+    side (local ids) and the face's nodes in the writing part's numbering, in the same order in both
+    parts' files.  ``pattern`` contains ``#``, replaced by the part index (the reference's
+    PARTITION_FILES convention).  Coordinates are written exactly.  Returns the file paths."""
+    from .solver import Mesh  # the global connectivity, in the reference's numbering
+
+    a = Mesh.from_raw(mesh).arrays()
+    n_cells = int(a["n_cells"])
+    f2c = a["face2cell"].reshape(-1, 2)
+    c2f_ptr, c2f = a["cell2face_ptr"], a["cell2face"]
+    f2n_ptr, f2n = a["face2node_ptr"], a["face2node"]
+    eptr, enodes = mesh.csr()
+    cx = np.array([mesh.xyz[enodes[eptr[e]:eptr[e + 1]], 0].mean() for e in range(n_cells)])
+    part = np.empty(n_cells, np.int64)
+    part[np.argsort(cx, kind="stable")] = np.arange(n_cells) * n_parts // n_cells
+    elems = [np.flatnonzero(part == p) for p in range(n_parts)]
+    g2l = np.empty(n_cells, np.int64)
+    for p in range(n_parts):
+        g2l[elems[p]] = np.arange(elems[p].size)
+    # local node numbering by first use over each part's elements
+    node_maps = []
+    for p in range(n_parts):
+        m = {}
+        for e in elems[p]:
+            for nd in enodes[eptr[e]:eptr[e + 1]]:
+                if int(nd) not in m:
+                    m[int(nd)] = len(m)
+        node_maps.append(m)
+    # boundary elements go with their interior element: match marker faces to boundary faces by node set
+    bface = {}
+    for f in range(int(a["n_faces_int"]), int(a["n_faces"])):
+        bface[frozenset(f2n[f2n_ptr[f]:f2n_ptr[f + 1]].tolist())] = int(f2c[f][0])
+    # inter-part faces in the order of the reference's loop (parts, local elements, element faces)
+    itf = [[[] for _ in range(n_parts)] for _ in range(n_parts)]
+    for p in range(n_parts):
+        for e in elems[p]:
+            for k in range(c2f_ptr[e], c2f_ptr[e + 1]):
+                f = c2f[k]
+                o = f2c[f][1] if f2c[f][0] == e else f2c[f][0]
+                if o >= n_cells or part[o] <= p:
+                    continue
+                q = int(part[o])
+                nodes = f2n[f2n_ptr[f]:f2n_ptr[f + 1]]
+                vtk = {3: 5, 4: 9}.get(len(nodes), 7)
+                itf[p][q].append([int(g2l[e]), int(g2l[o]), vtk] + [node_maps[p][int(x)] for x in nodes])
+                itf[q][p].append([int(g2l[o]), int(g2l[e]), vtk] + [node_maps[q][int(x)] for x in nodes])
+    paths = []
+    for p in range(n_parts):
+        path = pattern.replace("#", str(p))
+        nm = node_maps[p]
+        inv = np.empty(len(nm), np.int64)
+        for g, l in nm.items():
+            inv[l] = g
+        lines = ["%", "% Problem dimension", "%", "NDIME= 3", "%", "% Inner element connectivity", "%",
+                 f"NELEM= {elems[p].size}"]
+        for i, e in enumerate(elems[p]):
+            lines.append(f"{int(mesh.elem_vtk[e]):3d}" + "".join(f"{nm[int(x)]:10d}" for x in enodes[eptr[e]:eptr[e + 1]])
+                         + f"{i:10d}")
+        lines += ["%", "% Node coordinates", "%", f"NPOIN= {len(nm)}"]
+        for i, g in enumerate(inv):
+            lines.append("".join(f"{float(mesh.xyz[g, k])!r:>26}" for k in range(3)) + f"{i:10d}")
+        mk_lines, n_mk = [], 0
+        for mk in mesh.markers:
+            rows = []
+            for j in range(mk.vtk.size):
+                fn = mk.nodes[j][: NODES_PER_VTK[int(mk.vtk[j])]]
+                if part[bface[frozenset(fn.tolist())]] != p:
+                    continue
+                rows.append(f"{int(mk.vtk[j]):3d}" + "".join(f"{nm[int(x)]:10d}" for x in fn))
+            if rows:
+                n_mk += 1
+                mk_lines += [f"MARKER_TAG= {mk.tag}", f"MARKER_ELEMS= {len(rows)}"] + rows
+        lines += ["%", "% Boundary elements", "%", f"NMARK= {n_mk}"] + mk_lines
+        adj = [q for q in range(n_parts) if itf[p][q]]
+        lines += ["%", "% Internal Boundary elements", "%", f"NINTERNAL_MARKER= {len(adj)}"]
+        for q in adj:
+            lines += [f"INTERNAL_MARKER= {q}", f"NELEM_MPI= {len(itf[p][q])}"]
+            lines += ["".join(f"{v:10d}" for v in row) for row in itf[p][q]]
+        with open(path, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        paths.append(path)
+    return paths
+
+
 @dataclasses.dataclass
 class CaseConfig:
     """Flow and solver settings written into an ``.e3d`` file (src/parser/SimConfig.cpp:49-236)."""

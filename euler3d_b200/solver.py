@@ -49,6 +49,19 @@ class Mesh:
         return cls(h)
 
     @classmethod
+    def read_partitions(cls, paths: Sequence[str], cref: float = 1.0, threads: int = 0) -> "Mesh":
+        """The partition files of a multi-partition case merged into one mesh (e3d_mesh_read_partitions)."""
+        lib = _lib.load()
+        h = C.c_void_p()
+        arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
+        check(lib.e3d_mesh_read_partitions(arr, len(paths), cref, threads, C.byref(h)))
+        return cls(h)
+
+    def partition_cell_ptr(self) -> np.ndarray:
+        """First cell of each partition (and the cell count) for a mesh read from partition files."""
+        return self.array("partition_cell_ptr")
+
+    @classmethod
     def from_raw(cls, raw, cref: float = 1.0, threads: int = 0) -> "Mesh":
         """Prepare a :class:`euler3d_b200.meshgen.RawMesh` held in memory."""
         lib = _lib.load()

@@ -97,7 +97,8 @@ e3d_status e3d_mesh_info_get(const e3d_mesh *mesh, e3d_mesh_info *info);
 
 /* Read-only view of one prepared array by name: "face2cell", "cell2face_ptr", "cell2face",
  * "cell2cell", "face2node_ptr", "face2node", "face_normal", "face_unit_normal", "face_center",
- * "face_area", "cell_volume", "cell_centroid", "{wall,farfield,sym}_{ghost,interior,face}".
+ * "face_area", "cell_volume", "cell_centroid", "{wall,farfield,sym}_{ghost,interior,face}",
+ * "partition_cell_ptr" (empty unless read from partition files).
  * *is_double says whether the data is double (else int32).  Valid until e3d_mesh_destroy. */
 e3d_status e3d_mesh_array(const e3d_mesh *mesh, const char *name, const void **data, int64_t *count,
                           int32_t *is_double);
@@ -127,6 +128,15 @@ typedef struct e3d_mesh_desc {
 	int32_t n_sym;                    /* Mesh::GetSymmetry... */
 	const int32_t *sym_ghost, *sym_interior, *sym_face;
 } e3d_mesh_desc;
+
+/* The partition files of a multi-partition case (PARTITION_FILES= n, the .par files E3D_PRE writes,
+ * src/partition/Partition.cpp, read per rank by MeshPartition, src/parser/MeshPartition.cpp:39-112),
+ * merged into one mesh for one GPU: nodes shared by partitions are joined through the
+ * inter-partition faces (NINTERNAL_MARKER) both sides list, elements are concatenated partition by
+ * partition -- e3d_mesh_array "partition_cell_ptr" gives the first cell of each -- and boundary
+ * markers merged by tag.  Fails with E3D_ERR_MESH on inconsistent partitions. */
+e3d_status e3d_mesh_read_partitions(const char *const *paths, int32_t n_parts, double cref, int32_t n_threads,
+                                    e3d_mesh **out);
 
 /* <partition>.bry, WriteSolution::writeBoundaryFile (src/solver/WriteSolution.cpp:57-76): every wall
  * face's interior cell and node ids, byte for byte as the reference writes it. */

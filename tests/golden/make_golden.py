@@ -18,7 +18,10 @@ smoothing): the density RMS of every iteration and the final state.
 bump channel (``e3d_ref_driver outputs``, timings fixed at 1234 / 5678 ms): residuals.dat,
 cp_part_0.dat, summary.txt, mesh.par.sol and mesh.par.bry, with the run's settings in run.json.
 
-Run from the repository root:  python tests/golden/make_golden.py [integrators | outputs]
+``reference_partitions.npz`` holds the bytes of the reference's partitioned test case
+(test/mesh/StructuredBlock_8_p0..3.par) and of the mesh it was cut from.
+
+Run from the repository root:  python tests/golden/make_golden.py [integrators | outputs | partitions]
 """
 import os
 import shutil
@@ -145,6 +148,16 @@ def make_outputs(work):
                        "min_residual": min_res, "solver_ms": 1234, "total_ms": 5678}, f, indent=1)
 
 
+def make_reference_partitions(reference_root):
+    """The reference's own partitioned test case (test/mesh/StructuredBlock_8_p0..3.par, written by its
+    partitioner) and the mesh it was cut from, as file bytes."""
+    out = {}
+    d = os.path.join(reference_root, "test", "mesh")
+    for f in ["StructuredBlock_8.su2"] + [f"StructuredBlock_8_p{i}.par" for i in range(4)]:
+        out[f.replace(".", "_")] = np.frombuffer(open(os.path.join(d, f), "rb").read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "reference_partitions.npz"), **out)
+
+
 def make_reference_meshes(work, reference_root):
     out = {}
     for f in REFERENCE_TEST_MESHES:
@@ -175,6 +188,9 @@ def main():
         if sys.argv[1:] == ["outputs"]:
             make_outputs(work)
             return
+        if sys.argv[1:] == ["partitions"]:
+            make_reference_partitions(os.environ.get("E3D_REFERENCE_ROOT", "/root/reference"))
+            return
         make_outputs(work)
         print("integrators", make_integrators(work), "bytes")
         for name, n in GOLDEN_CASES.items():
@@ -182,6 +198,7 @@ def main():
         ref_root = os.environ.get("E3D_REFERENCE_ROOT", "/root/reference")
         if os.path.isdir(os.path.join(ref_root, "test", "mesh")):
             make_reference_meshes(work, ref_root)
+            make_reference_partitions(ref_root)
     finally:
         shutil.rmtree(work, ignore_errors=True)
 
