@@ -317,7 +317,8 @@ def run_reference(args, rank, world):
     n = min(args.n, 24)
     raw = meshgen.bump_box_tets(n)
     cells = raw.n_cells
-    K, W = max(args.steps // 5, 2), min(args.warmup, 2)
+    # each process runs ~10 s of reference solver iterations (about 0.1 s per RK5 iteration here)
+    K, W = max(2 * args.steps, 20), min(args.warmup, 2)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     procs = max(1, min(cores, 64))
     with tempfile.TemporaryDirectory(prefix="e3dref") as d:
@@ -332,8 +333,8 @@ def run_reference(args, rank, world):
             outs = [p.communicate()[0] for p in ps]
             secs = []
             for o in outs:
-                js = [ln for ln in o.splitlines() if ln.startswith("{")]
-                secs.append(json.loads(js[-1])["seconds"])
+                # the reference's last message has no newline: take the JSON object wherever it starts
+                secs.append(json.loads(o[o.rindex('{"cells"'):].splitlines()[0])["seconds"])
             wall = time.time() - t0
             tmax = max(secs)
             value = 5.0 * cells * K * procs / tmax

@@ -297,7 +297,9 @@ int main(int argc, char **argv) {
 		auto a = std::chrono::steady_clock::now();
 		solver.Run();
 		double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
-		std::printf("{\"cells\": %d, \"iterations\": %d, \"seconds\": %.9g, \"warm_seconds\": %.9g, \"setup_seconds\": %.6g}\n",
+		std::fflush(stdout);
+		std::cout << std::flush;
+		std::printf("\n{\"cells\": %d, \"iterations\": %d, \"seconds\": %.9g, \"warm_seconds\": %.9g, \"setup_seconds\": %.6g}\n",
 		            localmesh.GetnElemTot(), solver._nbInteration, s, warmSeconds, setupSeconds);
 		return 0;
 	}
