@@ -63,13 +63,14 @@ def served_leg(args) -> dict:
     """The served-stream comparison: a seeded Poisson stream of solve requests (bump-channel and
     biconvex O-grid meshes, log-uniform cell counts, Mach 0.3-0.85, AoA -4..6 deg, Roe or AUSM,
     residual-drop tolerance 1e-6 or 1e-8, at most ``served_max_iter`` iterations each) served with
-    continuous batching in FP64, then the same stream solved one at a time (plain FP64 path)."""
+    continuous batching in FP64 and with the FP32 -> FP64 precision ladder, then the same stream solved
+    one at a time (plain FP64 path)."""
     from euler3d_b200 import _lib, serve
 
     lo, hi = args.served_cells
     reqs = serve.request_stream(args.served_requests, args.served_rate, cells=(lo, hi), seed=4,
                                 drops=(1e-6, 1e-8), schemes=(_lib.SCHEME_ROE, _lib.SCHEME_AUSM))
-    out = serve.compare(reqs, _lib.PREC_FP64, max_iter=args.served_max_iter)
+    out = serve.compare(reqs, _lib.PREC_FP64, max_iter=args.served_max_iter, ladder=True)
     out["workload"] = (f"{args.served_requests} requests, Poisson {args.served_rate:g}/s (seed 4), "
                        f"cells log-uniform [{lo}, {hi}], Mach 0.3-0.85, AoA -4..6, Roe/AUSM, drop 1e-6/1e-8, "
                        f"max_iter {args.served_max_iter}")

@@ -17,7 +17,7 @@ SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
 ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE, KERNEL_TILE_B3 = 0, 1, 2, 3, 4, 5
-STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS = 0, 1, 2
+STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS, STOP_STALL = 0, 1, 2, 3
 INTEGRATOR_RK5, INTEGRATOR_EULER = 0, 1
 
 _dp = C.POINTER(C.c_double)
@@ -51,7 +51,7 @@ class FlowParams(C.Structure):
 class RunParams(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("sampling", C.c_int32), ("min_residual", C.c_double),
                 ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32),
-                ("stage_kernel", C.c_int32), ("min_residual_drop", C.c_double)]
+                ("stage_kernel", C.c_int32), ("min_residual_drop", C.c_double), ("stall_window", C.c_int32)]
 
 
 class RunStats(C.Structure):

@@ -51,6 +51,9 @@ struct Control {
     double rms0;       // RMS of the run's first iteration
     int n_samples;     // coefficient samples taken (residuals.dat rows)
     int sample_cap;    // capacity of the sample record
+    int stall_window;  // > 0: stop once the RMS has set no new minimum for this many iterations
+    int since_best;    // iterations since the RMS last set a new minimum
+    double best_rms;   // smallest RMS of the run so far
     double force[3], moment[3];
 };
 

@@ -57,6 +57,7 @@ class SolveResult:
     cm: float
     last_rms: float
     device_bytes: int
+    fp32_iterations: int = 0  # ladder: iterations of the FP32_FLUX phase
 
     @property
     def latency(self) -> float:
@@ -160,39 +161,59 @@ class Server:
 
     ``hbm_budget`` bounds the summed device memory of the admitted solves (an estimate reserved at
     admission, replaced by the handle's own figure once it exists); ``max_members`` bounds how many
-    run at once; ``iterations_per_step`` is the graph length between admissions and retirements."""
+    run at once; ``iterations_per_step`` is the graph length between admissions and retirements.
+
+    With ``ladder`` every solve runs first in FP32_FLUX (fluxes in single precision, about 1.7x the
+    FP64 throughput) until its tolerance or until its residual has set no new minimum for
+    ``stall_window`` iterations -- the floor single-precision fluxes put under the residual -- and
+    then continues in FP64 from that state to the same absolute residual the plain FP64 solve stops
+    at (the tolerance times the solve's first RMS).  The result is the FP64 solution."""
 
     def __init__(self, device: int = 0, precision: int = _lib.PREC_FP64, hbm_budget: float = 150e9,
                  max_members: int = 256, iterations_per_step: int = 32, max_iter: int = 200_000,
-                 prep_workers: int = 4, sampling: int = 1_000_000,
+                 prep_workers: int = 4, sampling: int = 1_000_000, ladder: bool = False, stall_window: int = 200,
                  clock: Callable[[], float] = time.perf_counter):
         self.device, self.precision = device, precision
         self.budget, self.max_members = float(hbm_budget), max_members
         self.every, self.max_iter, self.sampling = iterations_per_step, max_iter, sampling
         self.prep_workers, self.clock = prep_workers, clock
+        self.ladder, self.stall_window = ladder, stall_window
         self.peak_bytes = 0
         self.peak_members = 0
         self.steps = 0
         self.step_ms = 0.0
 
     def serve(self, requests: Sequence[SolveRequest], on_result: Optional[Callable] = None) -> List[SolveResult]:
+        first = _lib.PREC_FP32_FLUX if self.ladder else self.precision
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         prep = cf.ThreadPoolExecutor(self.prep_workers, thread_name_prefix="e3d-prep")
         device_pool = cf.ThreadPoolExecutor(1, thread_name_prefix="e3d-device")  # creation and release
         preparing = collections.deque()   # (req, future -> arrays)
         ready = collections.deque()       # (req, arrays, estimate)
-        creating = collections.deque()    # (req, future -> solver, estimate)
-        members: Dict[int, tuple] = {}    # id(solver) -> (req, solver, admitted, bytes)
+        creating = collections.deque()    # dicts: req, fut -> solver, est, phase, ...
+        members: Dict[int, dict] = {}     # id(solver) -> dict: req, solver, admitted, bytes, phase, ...
         results: List[SolveResult] = []
         used = 0.0
-        batch = Batch(self.device)
+        batches = [Batch(self.device)] + ([Batch(self.device)] if self.ladder else [])
+        steppers = cf.ThreadPoolExecutor(len(batches), thread_name_prefix="e3d-step")  # batches run concurrently
         t0 = self.clock()
         wake = threading.Event()
 
-        def create(req, arrays):
-            s = EulerSolver(arrays, request_flow(req, self.precision), autotune=False)
+        def create(req, arrays, prec, state=None):
+            s = EulerSolver(arrays, request_flow(req, prec), autotune=False)
+            if state is not None:
+                s.set_state(state)
             wake.set()
             return s
+
+        def finish(m, s, st, status, iterations, fp32_iterations):
+            req = m["req"]
+            cl, cd, cm = final_coefficients(s)
+            r = SolveResult(req.rid, s.n_cells, req.arrival, m["admitted"], self.clock() - t0, iterations,
+                            st["stop_reason"], status, cl, cd, cm, st["last_rms"], m["bytes"], fp32_iterations)
+            results.append(r)
+            if on_result:
+                on_result(r, s)
 
         try:
             while pending or preparing or ready or creating or members:
@@ -205,7 +226,7 @@ class Server:
                 while preparing and preparing[0][1].done():
                     req, fut = preparing.popleft()
                     arrays = fut.result()
-                    est = footprint_estimate(int(arrays["n_cells"]), int(arrays["n_faces"]), self.precision)
+                    est = footprint_estimate(int(arrays["n_cells"]), int(arrays["n_faces"]), first)
                     ready.append((req, arrays, est))
                 # admission by device-memory footprint, first come first served
                 while ready and len(members) + len(creating) < self.max_members:
@@ -220,39 +241,65 @@ class Server:
                         break
                     ready.popleft()
                     used += est
-                    creating.append((req, device_pool.submit(create, req, arrays), est))
-                while creating and creating[0][1].done():
-                    req, fut, est = creating.popleft()
-                    s = fut.result()
+                    creating.append({"req": req, "fut": device_pool.submit(create, req, arrays, first), "est": est,
+                                     "phase": 1, "arrays": arrays if self.ladder else None,
+                                     "admitted": self.clock() - t0})
+                while creating and creating[0]["fut"].done():
+                    c = creating.popleft()
+                    s = c["fut"].result()
                     nbytes = int(s.info()["device_bytes"])
-                    used += nbytes - est
-                    batch.add(s, max_iter=self.max_iter, sampling=self.sampling, min_residual_drop=req.drop)
-                    members[id(s)] = (req, s, self.clock() - t0, nbytes)
+                    used += nbytes - c["est"]
+                    m = dict(c, solver=s, bytes=nbytes)
+                    del m["fut"]
+                    req = c["req"]
+                    if c["phase"] == 1:
+                        m["admitted"] = self.clock() - t0
+                        batches[0].add(s, max_iter=self.max_iter, sampling=self.sampling, min_residual_drop=req.drop,
+                                       stall_window=self.stall_window if self.ladder else 0)
+                    else:
+                        batches[1].add(s, max_iter=max(self.max_iter - c["it1"], 0), sampling=self.sampling,
+                                       min_residual=c["rms0"] * req.drop)
+                    members[id(s)] = m
                 self.peak_bytes = max(self.peak_bytes, used)
                 self.peak_members = max(self.peak_members, len(members))
                 if members:
-                    batch.step(self.every)
-                    self.steps += 1
-                    self.step_ms += batch.info()["last_step_ms"]
-                    for s, st, status in batch.retire():
-                        req, _, admitted, nbytes = members.pop(id(s))
-                        finished = self.clock() - t0
-                        cl, cd, cm = final_coefficients(s)
-                        r = SolveResult(req.rid, s.n_cells, req.arrival, admitted, finished, st["iterations"],
-                                        st["stop_reason"], status, cl, cd, cm, st["last_rms"], nbytes)
-                        results.append(r)
-                        if on_result:
-                            on_result(r, s)
-                        used -= nbytes
-                        device_pool.submit(s.close)
+                    # each batch on its own stream: the ladder's two batches overlap on the device
+                    running = [b for b in batches if b.info()["n_running"]]
+                    for f in [steppers.submit(b.step, self.every) for b in running]:
+                        f.result()
+                    for b in running:
+                        self.steps += 1
+                        self.step_ms += b.info()["last_step_ms"]
+                    for phase, b in enumerate(batches, start=1):
+                        for s, st, status in b.retire():
+                            m = members.pop(id(s))
+                            if (phase == 1 and self.ladder and status == _lib.E3D_OK
+                                    and st["stop_reason"] == _lib.STOP_STALL):
+                                # FP32 floor reached: continue in FP64 from this state
+                                rms0 = float(s.rms_history()[0])
+                                state = s.get_state()
+                                est = footprint_estimate(s.n_cells, int(m["arrays"]["n_faces"]), _lib.PREC_FP64)
+                                used += est
+                                creating.append({"req": m["req"], "est": est, "phase": 2, "it1": st["iterations"],
+                                                 "rms0": rms0, "admitted": m["admitted"], "arrays": None,
+                                                 "fut": device_pool.submit(create, m["req"], m["arrays"],
+                                                                           _lib.PREC_FP64, state)})
+                            elif phase == 1:
+                                finish(m, s, st, status, st["iterations"], st["iterations"] if self.ladder else 0)
+                            else:
+                                finish(m, s, st, status, m["it1"] + st["iterations"], m["it1"])
+                            used -= m["bytes"]
+                            device_pool.submit(s.close)
                 else:
                     # idle: wait for the next arrival, a finished preparation or a created solver
                     wake.clear()
                     timeout = (pending[0].arrival - now) if pending else 0.05
-                    if not (preparing and preparing[0][1].done()) and not (creating and creating[0][1].done()):
+                    if not (preparing and preparing[0][1].done()) and not (creating and creating[0]["fut"].done()):
                         wake.wait(max(0.0, min(timeout, 0.05)))
         finally:
-            batch.close()
+            steppers.shutdown(wait=True)
+            for b in batches:
+                b.close()
             prep.shutdown(wait=True)
             device_pool.shutdown(wait=True)
         return results
@@ -292,7 +339,7 @@ def serve_plain(requests: Sequence[SolveRequest], device: int = 0, precision: in
             try:
                 st = s.run(max_iter, sampling=sampling, min_residual_drop=req.drop)
             except _lib.E3DError as e:
-                status, st = e.status, {"iterations": -1, "stop_reason": -1, "last_rms": math.nan}
+                status, st = e.status, getattr(e, "stats", {"iterations": -1, "stop_reason": -1, "last_rms": math.nan})
             finished = clock() - t0
             cl, cd, cm = final_coefficients(s)
             r = SolveResult(req.rid, s.n_cells, req.arrival, started, finished, st["iterations"],
@@ -308,11 +355,26 @@ def serve_plain(requests: Sequence[SolveRequest], device: int = 0, precision: in
     return results
 
 
+def _diffs(base: Sequence[SolveResult], other: Sequence[SolveResult]) -> Dict[str, object]:
+    by = {r.rid: r for r in other}
+    ok = [b for b in base if b.status == _lib.E3D_OK and by[b.rid].status == _lib.E3D_OK]
+    # relative to the coefficient's size, at least 1e-2 (a near-zero lift has no relative error)
+    dl = [abs(b.cl - by[b.rid].cl) / max(abs(b.cl), 1e-2) for b in ok]
+    dd = [abs(b.cd - by[b.rid].cd) / max(abs(b.cd), 1e-2) for b in ok]
+    mism = [b for b in base if (b.status, b.stop_reason) != (by[b.rid].status, by[b.rid].stop_reason)]
+    return {"max_rel_diff_cl": max(dl) if dl else None, "max_rel_diff_cd": max(dd) if dd else None,
+            "same_outcome": not mism,
+            "outcome_mismatches": [{"rid": b.rid, "cells": b.cells, "plain": [b.status, b.stop_reason, b.iterations],
+                                    "served": [by[b.rid].status, by[b.rid].stop_reason, by[b.rid].iterations]}
+                                   for b in mism]}
+
+
 def compare(requests: Sequence[SolveRequest], precision: int = _lib.PREC_FP64, iterations_per_step: int = 32,
             hbm_budget: float = 150e9, max_members: int = 256, prep_workers: int = 4,
-            plain: bool = True, max_iter: int = 200_000) -> Dict[str, object]:
-    """Serve ``requests`` with continuous batching, then (``plain``) the same stream one solve at a time
-    in FP64; solves/s, latency percentiles, and the largest lift / drag difference between the two."""
+            plain: bool = True, max_iter: int = 200_000, ladder: bool = False) -> Dict[str, object]:
+    """Serve ``requests`` with continuous batching (in ``precision``, and with ``ladder`` also with the
+    FP32 -> FP64 precision ladder), then (``plain``) the same stream one solve at a time in FP64;
+    solves/s, latency percentiles, and the largest lift / drag difference from the plain solves."""
     srv = Server(precision=precision, iterations_per_step=iterations_per_step, hbm_budget=hbm_budget,
                  max_members=max_members, prep_workers=prep_workers, max_iter=max_iter)
     served = srv.serve(requests)
@@ -321,22 +383,27 @@ def compare(requests: Sequence[SolveRequest], precision: int = _lib.PREC_FP64, i
                               "peak_members": srv.peak_members, "peak_device_bytes": srv.peak_bytes,
                               "device_busy_s": srv.step_ms / 1e3,
                               "failed": sum(r.status != _lib.E3D_OK for r in served)}
+    lad = None
+    if ladder:
+        ls = Server(iterations_per_step=iterations_per_step, hbm_budget=hbm_budget, max_members=max_members,
+                    prep_workers=prep_workers, max_iter=max_iter, ladder=True)
+        lad = ls.serve(requests)
+        out["served_ladder"] = summarize(lad)
+        out["served_ladder"]["fp32_iteration_share"] = (sum(r.fp32_iterations for r in lad) /
+                                                        max(sum(max(r.iterations, 0) for r in lad), 1))
+        out["served_ladder"]["device_busy_s"] = ls.step_ms / 1e3
     if plain:
         base = serve_plain(requests, prep_workers=prep_workers, max_iter=max_iter)
         out["plain"] = summarize(base)
-        by = {r.rid: r for r in served}
-        ok = [b for b in base if b.status == _lib.E3D_OK and by[b.rid].status == _lib.E3D_OK]
-        dl = [abs(b.cl - by[b.rid].cl) / max(abs(b.cl), 1e-3) for b in ok]
-        dd = [abs(b.cd - by[b.rid].cd) / max(abs(b.cd), 1e-3) for b in ok]
-        mism = [b for b in base if (b.status, b.stop_reason) != (by[b.rid].status, by[b.rid].stop_reason)]
-        out["same_outcome"] = not mism
-        out["outcome_mismatches"] = [{"rid": b.rid, "cells": b.cells, "plain": [b.status, b.stop_reason, b.iterations],
-                                      "served": [by[b.rid].status, by[b.rid].stop_reason, by[b.rid].iterations]}
-                                     for b in mism]
-        out["max_rel_diff_cl"] = max(dl) if dl else None
-        out["max_rel_diff_cd"] = max(dd) if dd else None
-        out["max_iteration_diff"] = max(abs(b.iterations - by[b.rid].iterations) for b in base) if base else None
+        out.update(_diffs(base, served))
+        out["max_iteration_diff"] = max(abs(b.iterations - r.iterations) for b, r in
+                                        zip(sorted(base, key=lambda r: r.rid), sorted(served, key=lambda r: r.rid)))
         out["speedup_solves_per_s"] = out["served"]["solves_per_s"] / out["plain"]["solves_per_s"]
+        if lad is not None:
+            d = _diffs(base, lad)
+            out["served_ladder"].update({k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "same_outcome")})
+            out["served_ladder"]["speedup_solves_per_s"] = (out["served_ladder"]["solves_per_s"] /
+                                                            out["plain"]["solves_per_s"])
     return out
 
 
@@ -356,6 +423,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--detail", action="store_true", help="print one line per served request")
     ap.add_argument("--max-iter", type=int, default=200_000)
+    ap.add_argument("--ladder", action="store_true", help="also serve with the FP32 -> FP64 precision ladder")
     a = ap.parse_args(argv)
     reqs = request_stream(a.requests, a.rate, cells=a.cells, seed=a.seed, drops=a.drops,
                           schemes=(_lib.SCHEME_ROE, _lib.SCHEME_AUSM))
@@ -369,8 +437,8 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
                               "stop": r.stop_reason, "status": r.status, "cl": r.cl, "cd": r.cd,
                               "latency_s": round(r.latency, 3), "last_rms": r.last_rms}), flush=True)
         return
-    print(json.dumps(compare(reqs, prec, a.every, a.budget_gb * 1e9, plain=not a.no_plain, max_iter=a.max_iter)),
-          flush=True)
+    print(json.dumps(compare(reqs, prec, a.every, a.budget_gb * 1e9, plain=not a.no_plain, max_iter=a.max_iter,
+                             ladder=a.ladder)), flush=True)
 
 
 if __name__ == "__main__":

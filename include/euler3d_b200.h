@@ -65,7 +65,7 @@ enum { E3D_ORDER_NATIVE = 0, E3D_ORDER_RCM = 1, E3D_ORDER_SPATIAL = 2 };
 enum { E3D_INTEGRATOR_RK5 = 0, E3D_INTEGRATOR_EULER = 1 };
 
 /* Why e3d_solver_run stopped (the exits of EulerSolver::Run, src/solver/EulerSolver.cpp:100-152). */
-enum { E3D_STOP_MAX_ITER = 0, E3D_STOP_RESIDUAL = 1, E3D_STOP_COEFFICIENTS = 2 };
+enum { E3D_STOP_MAX_ITER = 0, E3D_STOP_RESIDUAL = 1, E3D_STOP_COEFFICIENTS = 2, E3D_STOP_STALL = 3 };
 
 /* ------------------------------------------------------------------------------------------
  * Mesh preparation.  Replaces Mesh<MeshPartition>::solveConnectivity
@@ -215,6 +215,10 @@ typedef struct e3d_run_params {
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
 	                                     No counterpart in the reference, whose test is absolute. */
+	int32_t stall_window;             /* > 0: also stop (E3D_STOP_STALL) once the density RMS has set no
+	                                     new minimum for this many iterations -- the residual has hit
+	                                     the floor of the arithmetic (FP32_FLUX); 0 off.  No counterpart
+	                                     in the reference. */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {

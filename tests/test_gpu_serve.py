@@ -69,3 +69,29 @@ def test_oversized_request_is_refused():
     req = serve.request_stream(1, 0.0, cells=(2000, 2001), seed=1)
     res = serve.Server(hbm_budget=1e5).serve(req)
     assert len(res) == 1 and res[0].status == _lib.E3D_ERR_OOM
+
+
+def test_precision_ladder():
+    """FP32 flux first, FP64 from the FP32 floor to the tolerance: the same outcome as the plain FP64
+    solve, lift and drag within 1e-4 relative -- both stop at the same residual, from different
+    histories, so they agree as far as that residual converges the forces."""
+    reqs = stream()[:6]
+    lad = {r.rid: r for r in serve.Server(ladder=True, iterations_per_step=16, stall_window=100).serve(reqs)}
+    for req in reqs:
+        st, _, coeffs = solo(req)
+        r = lad[req.rid]
+        assert r.status == _lib.E3D_OK and r.stop_reason == st["stop_reason"] == _lib.STOP_RESIDUAL
+        assert r.fp32_iterations > 0
+        for a, b in zip((r.cl, r.cd), coeffs[:2]):
+            # relative to the coefficient scale: a near-zero lift is not a relative-error measure
+            assert abs(a - b) <= 1e-4 * max(abs(b), 1e-2), (req.rid, a, b)
+
+
+def test_stall_stop():
+    """An FP32 solve held to an unreachable tolerance stops on the stall test, not at max_iter."""
+    req = stream()[0]
+    s = EulerSolver(serve._prepare(req), serve.request_flow(req, _lib.PREC_FP32_FLUX), autotune=False)
+    st = s.run(100_000, sampling=1_000_000, min_residual_drop=1e-14, stall_window=100)
+    assert st["stop_reason"] == _lib.STOP_STALL and st["iterations"] < 100_000
+    h = s.rms_history()
+    assert np.min(h[-100:]) >= np.min(h[:-100])  # no new minimum in the last window
