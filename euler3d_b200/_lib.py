@@ -51,7 +51,8 @@ class FlowParams(C.Structure):
 class RunParams(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("sampling", C.c_int32), ("min_residual", C.c_double),
                 ("min_aerocoeff_error", C.c_double), ("check_every", C.c_int32), ("profile_stages", C.c_int32),
-                ("stage_kernel", C.c_int32), ("min_residual_drop", C.c_double), ("stall_window", C.c_int32)]
+                ("stage_kernel", C.c_int32), ("min_residual_drop", C.c_double), ("stall_window", C.c_int32),
+                ("stall_below", C.c_double)]
 
 
 class RunStats(C.Structure):

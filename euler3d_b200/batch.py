@@ -39,10 +39,11 @@ class Batch:
         return len(self._members)
 
     def add(self, solver: EulerSolver, max_iter: int, sampling: int = 1, min_residual: float = 0.0,
-            min_aerocoeff_error: float = 0.0, min_residual_drop: float = 0.0, stall_window: int = 0) -> None:
+            min_aerocoeff_error: float = 0.0, min_residual_drop: float = 0.0, stall_window: int = 0,
+            stall_below: float = 0.0) -> None:
         """Start a run of ``solver`` in the batch (stop criteria as in :meth:`EulerSolver.run`)."""
         rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, min_residual_drop=min_residual_drop,
-                        stall_window=stall_window)
+                        stall_window=stall_window, stall_below=stall_below)
         check(_lib.load().e3d_batch_add(self._h, solver._h, C.byref(rp)))
         self._members[solver._h.value] = solver
 

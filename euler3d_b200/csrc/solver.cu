@@ -56,8 +56,9 @@ __device__ __forceinline__ void finalize_body(const FinalizeArgs &f, double *sh)
         ctl->stop_reason = E3D_STOP_RESIDUAL;
         return;
     }
-    if (ctl->stall_window > 0) {  // the residual has stopped falling (a precision floor)
-        if (ctl->n_rms == 1 || rms < ctl->best_rms) {
+    if (ctl->stall_window > 0 && (ctl->stall_below <= 0.0 || rms < ctl->stall_below * ctl->rms0)) {
+        // the residual has stopped falling (a precision floor)
+        if (ctl->best_rms == 0.0 || rms < ctl->best_rms) {
             ctl->best_rms = rms;
             ctl->since_best = 0;
         } else if (++ctl->since_best >= ctl->stall_window) {
@@ -982,6 +983,7 @@ static void init_control(Solver *S, const e3d_run_params *rp, int max_iter, int 
     init.min_drop = rp->min_residual_drop;
     init.sample_cap = sample_cap;
     init.stall_window = std::max(rp->stall_window, 0);
+    init.stall_below = rp->stall_below;
     init.done = max_iter == 0;
     std::memcpy(S->ctl_host, &init, sizeof init);
     E3D_CUDA(cudaMemcpyAsync(S->ctl, S->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, s));

@@ -54,6 +54,7 @@ struct Control {
     int stall_window;  // > 0: stop once the RMS has set no new minimum for this many iterations
     int since_best;    // iterations since the RMS last set a new minimum
     double best_rms;   // smallest RMS of the run so far
+    double stall_below;  // the stall test counts only once RMS < stall_below x the first RMS (0: always)
     double force[3], moment[3];
 };
 

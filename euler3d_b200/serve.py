@@ -165,19 +165,21 @@ class Server:
 
     With ``ladder`` every solve runs first in FP32_FLUX (fluxes in single precision, about 1.7x the
     FP64 throughput) until its tolerance or until its residual has set no new minimum for
-    ``stall_window`` iterations -- the floor single-precision fluxes put under the residual -- and
+    ``stall_window`` iterations once it is below ``stall_below`` x its first value -- the floor
+    single-precision fluxes put under the residual; initial transients do not count -- and
     then continues in FP64 from that state to the same absolute residual the plain FP64 solve stops
     at (the tolerance times the solve's first RMS).  The result is the FP64 solution."""
 
     def __init__(self, device: int = 0, precision: int = _lib.PREC_FP64, hbm_budget: float = 150e9,
                  max_members: int = 256, iterations_per_step: int = 32, max_iter: int = 200_000,
                  prep_workers: int = 4, sampling: int = 1_000_000, ladder: bool = False, stall_window: int = 200,
+                 stall_below: float = 1e-2,
                  clock: Callable[[], float] = time.perf_counter):
         self.device, self.precision = device, precision
         self.budget, self.max_members = float(hbm_budget), max_members
         self.every, self.max_iter, self.sampling = iterations_per_step, max_iter, sampling
         self.prep_workers, self.clock = prep_workers, clock
-        self.ladder, self.stall_window = ladder, stall_window
+        self.ladder, self.stall_window, self.stall_below = ladder, stall_window, stall_below
         self.peak_bytes = 0
         self.peak_members = 0
         self.steps = 0
@@ -255,7 +257,8 @@ class Server:
                     if c["phase"] == 1:
                         m["admitted"] = self.clock() - t0
                         batches[0].add(s, max_iter=self.max_iter, sampling=self.sampling, min_residual_drop=req.drop,
-                                       stall_window=self.stall_window if self.ladder else 0)
+                                       stall_window=self.stall_window if self.ladder else 0,
+                                       stall_below=self.stall_below)
                     else:
                         batches[1].add(s, max_iter=max(self.max_iter - c["it1"], 0), sampling=self.sampling,
                                        min_residual=c["rms0"] * req.drop)

@@ -185,11 +185,11 @@ class FlowConfig:
 
 def run_params(max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
                check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
-               min_residual_drop: float = 0.0, stall_window: int = 0) -> _lib.RunParams:
+               min_residual_drop: float = 0.0, stall_window: int = 0, stall_below: float = 0.0) -> _lib.RunParams:
     """``e3d_run_params``: MAX_ITER, SAMPLING, MIN_RESIDUAL, MIN_AEROCOEFF_ERROR of the reference's
     config plus the launch options and the relative residual-drop stop."""
     return _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages),
-                          stage_kernel, min_residual_drop, stall_window)
+                          stage_kernel, min_residual_drop, stall_window, stall_below)
 
 
 def stats_dict(st: _lib.RunStats) -> Dict[str, object]:
@@ -264,9 +264,9 @@ class EulerSolver:
     # ---- hot path
     def run(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
             check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
-            min_residual_drop: float = 0.0, stall_window: int = 0) -> Dict[str, object]:
+            min_residual_drop: float = 0.0, stall_window: int = 0, stall_below: float = 0.0) -> Dict[str, object]:
         rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, profile_stages,
-                        stage_kernel, min_residual_drop, stall_window)
+                        stage_kernel, min_residual_drop, stall_window, stall_below)
         st = _lib.RunStats()
         status = _lib.load().e3d_solver_run(self._h, C.byref(rp), C.byref(st))
         stats = stats_dict(st)

@@ -219,6 +219,8 @@ typedef struct e3d_run_params {
 	                                     new minimum for this many iterations -- the residual has hit
 	                                     the floor of the arithmetic (FP32_FLUX); 0 off.  No counterpart
 	                                     in the reference. */
+	double stall_below;               /* > 0: the stall test starts once the RMS is below this fraction of
+	                                     the first RMS (initial transients do not count) */
 } e3d_run_params;
 
 typedef struct e3d_run_stats {
