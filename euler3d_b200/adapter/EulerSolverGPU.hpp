@@ -30,7 +30,8 @@ namespace E3D::Solver {
 class EulerSolverGPU {
 public:
     EulerSolverGPU(FlowField &flow, const E3D::Parallel::MPIHandler &mpi, const E3D::Mesh<E3D::Parser::MeshPartition> &mesh,
-                   const E3D::Parser::SimConfig &config, const E3D::Metrics &metrics, int precision = E3D_PREC_FP64)
+                   const E3D::Parser::SimConfig &config, const E3D::Metrics &metrics, int precision = E3D_PREC_FP64,
+                   bool useConfigScheme = false)
         : _flow(flow), _mpi(mpi), _mesh(mesh), _config(config) {
         if (mpi.getPoolSize() != 1) throw std::runtime_error("EulerSolverGPU runs one whole mesh per GPU (one partition)");
         const int nCells = mesh.GetnElemTot(), nFaces = mesh.GetnFace();
@@ -85,7 +86,12 @@ public:
         p.cd_sign = config.getMeshOrientationCD().second;
         p.cm_axis = config.getMeshOrientationCM().first;
         p.cm_sign = config.getMeshOrientationCM().second;
-        p.scheme = config.getSolverScheme() == E3D::Parser::SimConfig::SolverScheme::AUSM ? E3D_SCHEME_AUSM : E3D_SCHEME_ROE;
+        // The reference parses SCHEME= but never reads it: it always runs Roe (Solver::AUSM is declared,
+        // include/solver/ConvectiveFluxesSchemes.h:27-30, and never defined or called).  The same by
+        // default; useConfigScheme runs AUSM for SCHEME= 1.
+        p.scheme = useConfigScheme && config.getSolverScheme() == E3D::Parser::SimConfig::SolverScheme::AUSM
+                       ? E3D_SCHEME_AUSM
+                       : E3D_SCHEME_ROE;
         p.precision = precision;
         p.ordering = E3D_ORDER_SPATIAL;
         // TIME_INTEGRATION= (EulerSolver's constructor, src/solver/EulerSolver.cpp:49-56); the
