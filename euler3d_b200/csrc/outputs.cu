@@ -59,8 +59,41 @@ std::string toml_float(double v) {
     return s;
 }
 
+// The width toml++ 2.3.1 estimates for a double (extern/toml++/toml_default_formatter.hpp:129-143):
+// 3 for zero, else 2 + [v < 0] + size_t(log10|v|) + 1, in size_t arithmetic.  For |v| < 1 the
+// logarithm is negative and its conversion to size_t wraps the way x86-64 code converts it (the
+// truncated value taken as a signed 64-bit integer), so small magnitudes give "negative" widths.
+// NaN converts to 2^63 and +inf to 0 there.
+uint64_t toml_float_columns(double v) {
+    if (v == 0.0) return 3;
+    uint64_t w = 2;
+    if (v < 0.0) {
+        w += 1;
+        v = -v;
+    }
+    const double l = std::log10(v);
+    uint64_t c;
+    if (std::isnan(l)) c = uint64_t(1) << 63;
+    else if (std::isinf(l)) c = l > 0 ? 0 : uint64_t(1) << 63;
+    else c = (uint64_t)(int64_t)l;
+    return w + c + 1;
+}
+
+// A 3-vector as toml++ prints an array (toml_default_formatter.h:116-173): inline "[ a, b, c ]"
+// unless the estimated inline width reaches the 120-column wrap (toml_default_formatter.hpp:93-106,
+// 158-161; the running sum stops at the first partial sum that reaches 120 as an unsigned number,
+// and the arrays here sit one indent level below the root, so the column bias is 0).  Multi-line
+// arrays put each element on its own line, indented four spaces, and "]" on a line of its own.
 std::string toml_vec(const double v[3]) {
-    return "[ " + toml_float(v[0]) + ", " + toml_float(v[1]) + ", " + toml_float(v[2]) + " ]";
+    uint64_t width = 3;
+    for (int k = 0; k < 3; k++) {
+        width += toml_float_columns(v[k]) + 2;
+        if (width >= 120) break;
+    }
+    if (width < 120) return "[ " + toml_float(v[0]) + ", " + toml_float(v[1]) + ", " + toml_float(v[2]) + " ]";
+    std::string s = "[";
+    for (int k = 0; k < 3; k++) s += std::string(k ? "," : "") + "\n    " + toml_float(v[k]);
+    return s + "\n]";
 }
 
 // The last run's coefficient samples: 7 doubles each (iteration, force, moment).

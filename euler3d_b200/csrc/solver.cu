@@ -29,15 +29,24 @@ namespace e3d {
 __device__ __forceinline__ void finalize_body(const FinalizeArgs &f, double *sh) {
     Control *ctl = f.ctl;
     if (ctl->done) return;
-    double v = 0.0;
-    for (int i = threadIdx.x; i < f.n_part; i += kReduceThreads) v += f.partials[i];
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    if (f.rsq) {
+        // FP64_EXACT: EulerSolver::computeRMS's own order, one running sum over the cells in
+        // reference order (src/solver/EulerSolver.cpp:382-389)
+        if (threadIdx.x != 0) return;
+        double s = 0.0;
+        for (int i = 0; i < f.n_cells; i++) s += f.rsq[i];
+        sh[0] = s;
+    } else {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < f.n_part; i += kReduceThreads) v += f.partials[i];
+        sh[threadIdx.x] = v;
         __syncthreads();
+        for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x != 0) return;
     }
-    if (threadIdx.x != 0) return;
     double rms = sqrt(sh[0] / f.n_domain);
     if (ctl->n_rms < ctl->hist_cap) f.hist[ctl->n_rms] = rms;
     if (ctl->n_rms == 0) ctl->rms0 = rms;
@@ -876,6 +885,7 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     }
     S->w0_stride = (N + 31) / 32 * 32;
     S->w0.alloc(5 * (size_t)S->w0_stride);
+    if (p->precision == E3D_PREC_FP64_EXACT) S->rsq.alloc(N);
     if (p->residual_smoothing) {
         // interior neighbours of each device cell in the reference's element2face order (which is
         // its element2element order, src/connectivity/Connectivity.cpp:184-218), and 1 + 0.25 n

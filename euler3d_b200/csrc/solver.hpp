@@ -59,6 +59,8 @@ struct FinalizeArgs {
     double n_domain;         // interior cells
     double *hist;            // RMS history
     Control *ctl;
+    const double *rsq;       // FP64_EXACT: R_rho^2 per cell in reference order, summed sequentially
+    int n_cells;
 };
 
 // Residual smoothing (EulerSolver::smoothResiduals, src/solver/EulerSolver.cpp:483-518): one Jacobi
@@ -148,6 +150,7 @@ struct Solver {
     double wall_sum[3] = {0, 0, 0};
     std::vector<double> wall_center_host;
     DevBuf<int> nb_ptr, nb;
+    DevBuf<double> rsq;                 // FP64_EXACT: per-cell R_rho^2 in reference order
     DevBuf<double> den, rbuf;
     DevBuf<unsigned long long> smooth_flags;
     Control *ctl = nullptr;        // device
@@ -186,6 +189,7 @@ struct Solver {
                                 &scratch, &den, &rbuf};
         nb_ptr.release();
         nb.release();
+        rsq.release();
         samples.release();
         wall_cp.release();
         smooth_flags.release();
@@ -204,7 +208,7 @@ struct Solver {
                (int64_t)tile_rec32_off.n * 8 +
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
-                         hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n + samples.n + wall_cp.n) * 8 +
+                         hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n + samples.n + wall_cp.n + rsq.n) * 8 +
                (int64_t)(nb_ptr.n + nb.n) * 4 + (int64_t)sizeof(Control);
     }
 
@@ -254,6 +258,7 @@ struct Solver {
         a.integrator = prm.integrator;
         a.split = 0;
         a.r_dev = nullptr;
+        a.rsq = rsq.p;
         return a;
     }
 
@@ -364,7 +369,7 @@ struct Solver {
     }
 
     FinalizeArgs finalize_args(const double *part, double *h) const {
-        return FinalizeArgs{part, n_blocks, (double)N, h, ctl};
+        return FinalizeArgs{part, n_blocks, (double)N, h, ctl, rsq.p, N};
     }
 
     bool euler() const { return prm.integrator == E3D_INTEGRATOR_EULER; }

@@ -108,6 +108,8 @@ struct StageArgs {
     int split;                       // residual phase of a split stage: write R to r_dev, no update
     double *__restrict__ r_dev;      // [5 x w0_stride] residual of a split stage (device order); the
                                      // update phase reads the smoothed residual from here
+    double *__restrict__ rsq;        // FP64_EXACT: R_rho^2 of every cell in reference order (last stage),
+                                     // summed sequentially like EulerSolver::computeRMS; else null
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -555,6 +557,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
 #pragma unroll
         for (int k = 0; k < 5; k++) a.w0[k * st + c] = W[k];
         a.ecell[c] = E;
+        if (a.rsq) a.rsq[a.new2old[c]] = R[0] * R[0];
         return R[0] * R[0];
     }
     // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
@@ -564,6 +567,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
     a.w0[3 * st + c] = s.w * s.rho;
     a.w0[4 * st + c] = E * s.rho;
     a.ecell[c] = E;
+    if (a.rsq) a.rsq[a.new2old[c]] = R[0] * R[0];
     return R[0] * R[0];
 }
 

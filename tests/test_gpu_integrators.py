@@ -1,9 +1,9 @@
 """Explicit Euler (TIME_INTEGRATION= 0) and residual smoothing (RESIDUAL_SMOOTHING= 1) on the GPU,
 against the oracle (itself pinned bit for bit to the reference, tests/test_oracle.py).
 
-FP64_EXACT must equal the oracle bit for bit for the state (ghost E of supersonic-outflow ghosts
-and the density RMS differ by summation order only, at most 1e-13 relative), with the same
-iteration counts; FP64 stays within 1e-10 relative per cell."""
+FP64_EXACT must equal the oracle bit for bit for the state and the density RMS (ghost E of
+supersonic-outflow ghosts differs in the last bit, at most 1e-13 relative), with the same iteration
+counts; FP64 stays within 1e-10 relative per cell."""
 import numpy as np
 import pytest
 
