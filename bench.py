@@ -288,9 +288,9 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": (["-", "-", "tile_kernel_f32<2>", "tile_kernel_f32<3>"] if args.precision == "fp32" else
-                                ["stage_kernel<false,2>", "stage_kernel<false,3>", "tile_kernel<false>",
-                                 "tile_pipe_kernel<false>", "tile_kernel<false,3>"])[solver.info()["stage_variant"]],
+                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_kernel_f32<6>"] if args.precision == "fp32" else
+                                ["stage_kernel<false,4>", "stage_kernel<false,5>", "tile_kernel<false,4>",
+                                 "tile_pipe_kernel<false>", "tile_kernel<false,7>"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "autotune": solver.info()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,

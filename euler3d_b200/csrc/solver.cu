@@ -600,8 +600,14 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
     if (!S->pipe_ok) S->pipe_smem = 0;
     if (!S->tiles_ok) return;
     cudaStream_t s = S->stream;
+    // halo lists at a fixed stride per tile, padded with -1: a block reads its entries without
+    // first reading where they start
+    S->halo_stride = std::max(max_halo, 1);
+    std::vector<int> halo_pad((size_t)n_tiles * S->halo_stride, -1);
+    for (int t = 0; t < n_tiles; t++)
+        std::copy(halo.begin() + halo_ptr[t], halo.begin() + halo_ptr[t + 1], halo_pad.begin() + (size_t)t * S->halo_stride);
     S->tile_halo_ptr.upload(halo_ptr, s);
-    S->tile_halo.upload(halo, s);
+    S->tile_halo.upload(halo_pad, s);
     S->tile_face_ptr.upload(face_ptr, s);
     S->tile_rec.upload(tface, s);
     S->tile_rec_off.upload(rec_off, s);
@@ -695,7 +701,6 @@ static void create_solver(const e3d_mesh_desc *d, const e3d_flow_params *p, Solv
     E3D_CUDA(cudaSetDevice(p->device));
     S->device = p->device;
     S->prm = *p;
-    S->prefetch_distance = 2 * prop.multiProcessorCount;  // two resident tile blocks per SM
     S->n_sm = prop.multiProcessorCount;
     if (p->stream) {
         S->stream = (cudaStream_t)p->stream;
@@ -1285,10 +1290,10 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
 // ---------------------------------------------------------------------------------------------
 // Allocation-free run.  The RMS partials and the RMS history of e3d_solver_run_noalloc live in this
 // file-scope device array instead of handle buffers, and the iterations are launched directly
-// (instantiating a CUDA graph allocates), so the call allocates no memory.  The array is 1 MiB,
+// (instantiating a CUDA graph allocates), so the call allocates no memory.  The array is 1.5 MiB,
 // exists on every device that loads the library until the process exits, and is shared by every
 // call: calls that overlap on the GPU race on it.
-constexpr int kNoAllocMaxBlocks = 65536;  // RMS partials -> at most 65536 x 256 = 16,777,216 cells
+constexpr int kNoAllocMaxBlocks = 131072;  // RMS partials -> at most 131072 x 128 = 16,777,216 cells
 constexpr int kNoAllocMaxIter = 65536;    // RMS history entries -> at most 65536 iterations per call
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + kNoAllocMaxIter];
 

@@ -19,7 +19,7 @@ void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
 void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_f32(size_t smem_bytes);
-// gather (two register budgets), face tiles, pipelined face tiles, face tiles at 3 blocks/SM
+// gather (two register budgets), face tiles, pipelined face tiles, face tiles at 7 blocks/SM
 constexpr int kStageVariants = 5;
 
 constexpr int kReduceThreads = 256;
@@ -129,7 +129,7 @@ struct Solver {
     size_t tile32_smem = 0;
     DevBuf<unsigned short> tile_contrib;
     int w0_stride = 0;
-    int prefetch_distance = 0;  // tile_kernel L2 prefetch distance: resident blocks on the device
+    int halo_stride = 0;        // entries per tile of tile_halo
     bool tiles_ok = false, pipe_ok = false;
     size_t pipe_smem = 0;
     int n_tiles = 0, n_sm = 0;
@@ -247,7 +247,7 @@ struct Solver {
         a.smem_faces = smem_faces;
         a.w0_stride = w0_stride;
         a.fault = &ctl->fault;
-        a.prefetch_distance = prefetch_distance;
+        a.halo_stride = halo_stride;
         a.n_tiles = n_tiles;
         a.pipe_grid = std::min(n_tiles, n_sm);
         a.q32in = q32[in_buf].p;
@@ -322,7 +322,7 @@ struct Solver {
         ghost_copy.release();
     }
 
-    // Without tuning: the face-tile kernel (three blocks per SM in FP64 and FP32_FLUX modes), or the
+    // Without tuning: the face-tile kernel (seven blocks per SM in FP64, six in FP32_FLUX), or the
     // gather kernel when the mesh does not fit the tiles.
     void use_default_variant() {
         for (auto &m : variant_ms) m = -1.0f;

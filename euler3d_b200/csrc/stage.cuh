@@ -25,7 +25,11 @@ namespace e3d {
 
 enum : int { TAG_LEFT = 0, TAG_RIGHT = 1, TAG_WALL = 2, TAG_SYM = 3, TAG_FAR = 4, TAG_FROZEN = 5 };
 constexpr int kTagBits = 3;
-constexpr int kStageThreads = 256;
+// Threads per block of the stage kernels, and cells per face tile.  Of tiles of 64, 128 and 256
+// cells, 128 ran the FP64 tile stage fastest on B200 (12.6M tetrahedra: 0.97, 0.85 and 0.93 ms):
+// more, smaller blocks per SM interleave their load and compute phases better, until the halo
+// share of smaller tiles costs more than that gains.
+constexpr int kStageThreads = 128;
 constexpr int kTileCells = kStageThreads;   // cells owned by one face tile (one per thread)
 constexpr int kTileLocalBits = 10;          // local (owned + halo) cell index in a tile face entry
 constexpr unsigned short kNoContrib = 0xFFFF;
@@ -84,8 +88,8 @@ struct StageArgs {
     int w0_stride;                   // row stride of w0
     // face-tile kernel: tile t owns cells [t*kTileCells, ...); its halo cells, face records and
     // the per-cell contribution lists (see tile_kernel)
-    const int *__restrict__ tile_halo_ptr;
-    const int *__restrict__ tile_halo;
+    const int *__restrict__ tile_halo_ptr;   // halo count of tile t = ptr[t+1] - ptr[t]
+    const int *__restrict__ tile_halo;       // halo cells of tile t at [t * halo_stride, ...), then -1
     const int *__restrict__ tile_face_ptr;   // face count of tile t = ptr[t+1] - ptr[t]
     const char *__restrict__ tile_rec;       // FaceRec blocks, one 16-byte aligned block per tile
     const long long *__restrict__ tile_rec_off;  // byte offset of tile t's block
@@ -94,7 +98,7 @@ struct StageArgs {
     int smem_cells;                  // max owned + halo cells of a tile
     int smem_faces;                  // max faces of a tile
     int *fault;                      // set when a bounded wait gives up (reported as a timeout)
-    int prefetch_distance;           // tile_kernel: tiles ahead whose data each block prefetches into L2
+    int halo_stride;                 // entries per tile in tile_halo (the largest halo)
     int n_tiles;                     // tiles of the mesh
     int pipe_grid;                   // tile_pipe_kernel: persistent blocks (one per SM)
     // FP32_FLUX mode: float cell records (rho,u,v,w | p,H,sqrt(rho),rsqrt(gamma p rho)), float
@@ -238,23 +242,26 @@ __device__ __forceinline__ void roe_exact(const Prim &L, const Prim &R, double n
 // Fast: the same flux rearranged as F = (F_L + F_R - sum_k a_k r_k) / 2 with the wave strengths
 // a_k formed once, Roe weights from one reciprocal, c~ and 1/c~^2 from one rsqrt, and the left
 // sound speed from rsqrt(gamma p rho).  sl, sr = sqrt(rho) and rcl = rsqrt(gamma p_L rho_L) come
-// from the caller (each is computed once per cell where possible).
+// from the caller (the gather kernel computes them once per cell, the tile kernels once per face).
+// The FP64 kernels are compiled without multiply-add contraction and fuse where the source says
+// fma(), so the rounding is fixed by the source: every kernel variant, alone or batched, computes
+// the same bits whatever its register budget.
 __device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl, double sr, double rcl,
                                          double nx, double ny, double nz, double g, double F[5]) {
     double inv = rcp_nr(sl + sr);
     double wl = sl * inv, wr = sr * inv;
-    double ut = L.u * wl + R.u * wr;
-    double vt = L.v * wl + R.v * wr;
-    double wt = L.w * wl + R.w * wr;
-    double ht = L.H * wl + R.H * wr;
+    double ut = fma(L.u, wl, R.u * wr);
+    double vt = fma(L.v, wl, R.v * wr);
+    double wt = fma(L.w, wl, R.w * wr);
+    double ht = fma(L.H, wl, R.H * wr);
     double rt = sl * sr;
-    double q2t = ut * ut + vt * vt + wt * wt;
-    double c2 = (g - 1.0) * (ht - 0.5 * q2t);
+    double q2t = fma(ut, ut, fma(vt, vt, wt * wt));
+    double c2 = (g - 1.0) * fma(-0.5, q2t, ht);
     double rc = rsqrt_nr(c2);
     double ct = c2 * rc, ic2 = rc * rc;
-    double Vt = ut * nx + vt * ny + wt * nz;
-    double Vl = L.u * nx + L.v * ny + L.w * nz;
-    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    double Vt = fma(ut, nx, fma(vt, ny, wt * nz));
+    double Vl = fma(L.u, nx, fma(L.v, ny, L.w * nz));
+    double Vr = fma(R.u, nx, fma(R.v, ny, R.w * nz));
     double drho = R.rho - L.rho, dp = R.p - L.p, dV = Vr - Vl;
     double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
     // Harten's fix with delta = c_L / 15 (c_L = gamma p_L * rsqrt(gamma p_L rho_L))
@@ -263,23 +270,23 @@ __device__ __forceinline__ void roe_fast(const Prim &L, const Prim &R, double sl
     double lam1 = fabs(Vt - ct), lam5 = fabs(Vt + ct);
     if (!(lam1 > delta) || !(lam5 > delta)) {
         double h = 7.5 * (L.rho * rcl);  // 1 / (2 delta)
-        if (!(lam1 > delta)) lam1 = (lam1 * lam1 + delta * delta) * h;
-        if (!(lam5 > delta)) lam5 = (lam5 * lam5 + delta * delta) * h;
+        if (!(lam1 > delta)) lam1 = fma(lam1, lam1, delta * delta) * h;
+        if (!(lam5 > delta)) lam5 = fma(lam5, lam5, delta * delta) * h;
     }
     double rcdv = rt * ct * dV;
     double a1 = 0.5 * lam1 * (dp - rcdv) * ic2;
     double a5 = 0.5 * lam5 * (dp + rcdv) * ic2;
     double aV = fabs(Vt);
-    double a2 = aV * (drho - dp * ic2);
+    double a2 = aV * fma(-dp, ic2, drho);
     double a3 = aV * rt;
     double a15 = a1 + a5, d51 = (a5 - a1) * ct, asum = a15 + a2;
-    double mL = L.rho * Vl, mR = R.rho * Vr;
+    double mL = L.rho * Vl, mR = R.rho * Vr, pp = L.p + R.p;
     F[0] = 0.5 * (mL + mR - asum);
-    F[1] = 0.5 * (mL * L.u + mR * R.u + (L.p + R.p) * nx - (asum * ut + d51 * nx + a3 * (du - dV * nx)));
-    F[2] = 0.5 * (mL * L.v + mR * R.v + (L.p + R.p) * ny - (asum * vt + d51 * ny + a3 * (dv - dV * ny)));
-    F[3] = 0.5 * (mL * L.w + mR * R.w + (L.p + R.p) * nz - (asum * wt + d51 * nz + a3 * (dw - dV * nz)));
-    F[4] = 0.5 * (mL * L.H + mR * R.H -
-                  (a15 * ht + d51 * Vt + a2 * (0.5 * q2t) + a3 * (ut * du + vt * dv + wt * dw - Vt * dV)));
+    F[1] = 0.5 * (fma(mL, L.u, fma(mR, R.u, pp * nx)) - fma(asum, ut, fma(d51, nx, a3 * fma(-dV, nx, du))));
+    F[2] = 0.5 * (fma(mL, L.v, fma(mR, R.v, pp * ny)) - fma(asum, vt, fma(d51, ny, a3 * fma(-dV, ny, dv))));
+    F[3] = 0.5 * (fma(mL, L.w, fma(mR, R.w, pp * nz)) - fma(asum, wt, fma(d51, nz, a3 * fma(-dV, nz, dw))));
+    F[4] = 0.5 * (fma(mL, L.H, mR * R.H) -
+                  fma(a15, ht, fma(d51, Vt, fma(a2, 0.5 * q2t, a3 * fma(-Vt, dV, fma(ut, du, fma(vt, dv, wt * dw)))))));
 }
 
 // ------------------------------------------------------------------------------ AUSM flux
@@ -336,8 +343,8 @@ __device__ __forceinline__ void ausm_fast(const Prim &L, const Prim &R, double r
                                           double nz, double g, double F[5]) {
     // c = gamma p / sqrt(gamma p rho); 1/c = rho / sqrt(gamma p rho)
     double cl = g * L.p * rl, cr = g * R.p * rr;
-    double Vl = L.u * nx + L.v * ny + L.w * nz;
-    double Vr = R.u * nx + R.v * ny + R.w * nz;
+    double Vl = fma(L.u, nx, fma(L.v, ny, L.w * nz));
+    double Vr = fma(R.u, nx, fma(R.v, ny, R.w * nz));
     ausm_tail(L, R, cl, cr, Vl, Vr, Vl * (L.rho * rl), Vr * (R.rho * rr), nx, ny, nz, F);
 }
 
@@ -492,7 +499,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         dt = a.cfl * cg.w / lam;
     } else {
         double snd = g * me.p * r_me;
-        lam = 0.5 * ((fabs(me.u) + snd) * cg.x + (fabs(me.v) + snd) * cg.y + (fabs(me.w) + snd) * cg.z);
+        lam = 0.5 * fma(fabs(me.u) + snd, cg.x, fma(fabs(me.v) + snd, cg.y, (fabs(me.w) + snd) * cg.z));
         dt = a.residual_only ? a.cfl * cg.w / lam : 0.0;  // the update below needs only alpha*cfl/lam
     }
     if (a.residual_only) {
@@ -519,7 +526,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         } else {
             const double coef = a.cfl * rcp_nr(lam);  // dt / V
 #pragma unroll
-            for (int k = 0; k < 5; k++) W[k] = W0[k] - coef * R[k];
+            for (int k = 0; k < 5; k++) W[k] = fma(-coef, R[k], W0[k]);
         }
     } else if (EXACT) {
         // W = W0 - alpha dt R / V and primitive recovery (EulerSolver.cpp:461-470, FlowField.cpp:140-171)
@@ -528,7 +535,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
     } else {
         double coef = a.alpha * a.cfl * rcp_nr(lam);  // alpha dt / V
 #pragma unroll
-        for (int k = 0; k < 5; k++) W[k] = W0[k] - coef * R[k];
+        for (int k = 0; k < 5; k++) W[k] = fma(-coef, R[k], W0[k]);
     }
     Prim s;
     double E;
@@ -547,7 +554,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         s.v = W[2] * ir;
         s.w = W[3] * ir;
         E = W[4] * ir;
-        s.p = (g - 1.0) * (W[4] - 0.5 * (W[1] * s.u + W[2] * s.v + W[3] * s.w));
+        s.p = (g - 1.0) * fma(-0.5, fma(W[1], s.u, fma(W[2], s.v, W[3] * s.w)), W[4]);
         s.H = (W[4] + s.p) * ir;
     }
     store_prim(a.qout, c, s);
@@ -699,9 +706,11 @@ __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15
 //   st[LC]   48-byte states: owned cells (one bulk copy) then halo cells (outside neighbours,
 //            gathered with cp.async)
 //   rec[FC]  FaceRec of every face touching the tile (one bulk copy)
-//   cg[T], ct[MC][T]   cell geometry and contribution lists (bulk copies)
-// W0 (only ever read by the thread that owns the cell) stays in global memory: its rows are
-// prefetched into L2 when the tile starts and read, coalesced, by the update.
+//   ct[MC][T]   contribution lists (one bulk copy)
+// W0 and the cell geometry (only ever read by the thread that owns the cell) stay in global
+// memory: their rows are prefetched into L2 when the tile starts and read, coalesced, into
+// registers before the flux phase ends.  Keeping them out of shared memory lets seven blocks share
+// an SM.
 // Evaluation: every face touching the tile is evaluated once (a face shared with another tile is
 // evaluated by both) and its F*S (5 doubles, 40 bytes) written over the face's own 40-byte record,
 // which only the thread evaluating the face reads; each cell then sums its faces' F*S in ascending
@@ -710,39 +719,38 @@ __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15
 struct TileBuf {
     double2 *st;
     FaceRec *rec;
-    double4 *cg;
     unsigned short *ct;
 };
 
 __host__ __device__ __forceinline__ size_t tile_buf_bytes(int LC, int FC, int MC) {
-    return (size_t)LC * 48 + ((40u * (size_t)FC + 15) & ~(size_t)15) + kTileCells * 32 + (size_t)MC * kTileCells * 2;
+    return (size_t)LC * 48 + ((40u * (size_t)FC + 15) & ~(size_t)15) + (size_t)MC * kTileCells * 2;
 }
 
 __device__ __forceinline__ TileBuf tile_buf_at(unsigned char *base, int LC, int FC, int MC) {
     TileBuf b;
     b.st = reinterpret_cast<double2 *>(base);
     b.rec = reinterpret_cast<FaceRec *>(base + (size_t)LC * 48);
-    b.cg = reinterpret_cast<double4 *>(base + (size_t)LC * 48 + round16(40u * FC));
-    b.ct = reinterpret_cast<unsigned short *>(b.cg + kTileCells);
+    b.ct = reinterpret_cast<unsigned short *>(base + (size_t)LC * 48 + round16(40u * FC));
     return b;
 }
 
-// Thread `lead` issues the tile's bulk copies onto bar (expecting their byte count).
-__device__ __forceinline__ void tile_issue_bulk(const StageArgs &a, int tile, const TileBuf &b, uint64_t *bar) {
+// One thread issues the tile's bulk copies onto bar (expecting their byte count); nf and rec_off are
+// the tile's face count and record offset.
+__device__ __forceinline__ void tile_issue_bulk(const StageArgs &a, int tile, int nf, long long rec_off,
+                                                const TileBuf &b, uint64_t *bar) {
     const int T = kTileCells, MC = a.max_contrib;
     const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
     const uint32_t b_state = (uint32_t)nloc * 48u;
     const uint32_t b_rec = round16(40u * (uint32_t)nf);
     const uint32_t b_w0 = round16((uint32_t)nloc * 8u);  // stays inside the padded rows
     const uint32_t b_cg = (uint32_t)nloc * 32u;
     const uint32_t b_ct = (uint32_t)MC * T * 2u;
-    mbar_expect_tx(bar, b_state + b_rec + b_cg + b_ct);
+    mbar_expect_tx(bar, b_state + b_rec + b_ct);
     bulk_g2s(b.st, a.qin + 3 * (size_t)c0, b_state, bar);
-    bulk_g2s(b.rec, a.tile_rec + a.tile_rec_off[tile], b_rec, bar);
-    for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
-    bulk_g2s(b.cg, a.cgeo + c0, b_cg, bar);
+    bulk_g2s(b.rec, a.tile_rec + rec_off, b_rec, bar);
     bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+    for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
+    bulk_prefetch_l2(a.cgeo + c0, b_cg);
 }
 
 // Halo state i of the tile (global cell h) into st[nloc + i] with three 16-byte cp.async.
@@ -759,20 +767,12 @@ __device__ __forceinline__ Prim tile_prim(const double2 *st, int i) {
     return Prim{x.x, x.y, y.x, y.y, z.x, z.y};
 }
 
-// sqrt(rho) and rsqrt(gamma p rho) of the tile's cells (fast path only).
-template <int NT>
-__device__ __forceinline__ void tile_roots(const StageArgs &a, const TileBuf &b, double *sq, int LC, int ncells) {
-    for (int i = threadIdx.x; i < ncells; i += NT) {
-        const Prim q = tile_prim(b.st, i);
-        sq[i] = q.rho * rsqrt_nr(q.rho);
-        sq[LC + i] = rsqrt_nr(a.gamma * q.p * q.rho);
-    }
-}
-
-// One flux per tile face; F*S of face j replaces record j (fs[5 j + k] aliases b.rec[j]).
+// One flux per tile face; F*S of face j replaces record j (fs[5 j + k] aliases b.rec[j]).  The fast
+// path takes sqrt(rho) and rsqrt(gamma p rho) of both sides per face: a per-cell pass over the tile
+// before the fluxes would cost a barrier phase and 16 bytes of shared memory per local cell, and
+// measured slower on B200.
 template <bool EXACT, int NT>
-__device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, const double *sq, double *fs,
-                                            int LC, int FC, int nf, int c0) {
+__device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, double *fs, int nf, int c0) {
     const double g = a.gamma;
     for (int j = threadIdx.x; j < nf; j += NT) {
         const FaceRec fr = b.rec[j];
@@ -786,21 +786,30 @@ __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b
             const Prim R = tile_prim(b.st, r);
             if (a.scheme == 1) {
                 if (EXACT) ausm_exact(L, R, fg.x, fg.y, fg.z, g, F);
-                else ausm_fast(L, R, sq[LC + l], sq[LC + r], fg.x, fg.y, fg.z, g, F);
+                else ausm_fast(L, R, rsqrt_nr(g * L.p * L.rho), rsqrt_nr(g * R.p * R.rho), fg.x, fg.y, fg.z, g, F);
             } else {
                 if (EXACT) roe_exact(L, R, fg.x, fg.y, fg.z, g, F);
-                else roe_fast(L, R, sq[l], sq[r], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                else
+                    roe_fast(L, R, L.rho * rsqrt_nr(L.rho), R.rho * rsqrt_nr(R.rho), rsqrt_nr(g * L.p * L.rho), fg.x,
+                             fg.y, fg.z, g, F);
             }
         } else {
             Prim gs;
             double *gp = a.ghost + 8 * (size_t)fr.ghost;
             if (boundary_face(a, tag, gp, c0 + l, L, fg, F, gs)) {
+                // the ghost's density and pressure are the interior cell's (mirror)
                 if (a.scheme == 1) {
                     if (EXACT) ausm_exact(L, gs, fg.x, fg.y, fg.z, g, F);
-                    else ausm_fast(L, gs, sq[LC + l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                    else {
+                        const double rl = rsqrt_nr(g * L.p * L.rho);
+                        ausm_fast(L, gs, rl, rl, fg.x, fg.y, fg.z, g, F);
+                    }
                 } else {
                     if (EXACT) roe_exact(L, gs, fg.x, fg.y, fg.z, g, F);
-                    else roe_fast(L, gs, sq[l], sq[l], sq[LC + l], fg.x, fg.y, fg.z, g, F);
+                    else {
+                        const double sl = L.rho * rsqrt_nr(L.rho);
+                        roe_fast(L, gs, sl, sl, rsqrt_nr(g * L.p * L.rho), fg.x, fg.y, fg.z, g, F);
+                    }
                 }
             }
         }
@@ -811,20 +820,24 @@ __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b
     }
 }
 
+// W0 and geometry of owned cell i (global memory, prefetched into L2 when the tile started).
+__device__ __forceinline__ void tile_load_cell(const StageArgs &a, int c0, int i, double W0[5], double4 &cg) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
+    cg = a.cgeo[c0 + i];
+}
+
 // Cell i of the tile: sum of its contributions, then time step and update; returns R_rho^2 on
-// the last stage.  The contribution entries and W0 / geometry loads are issued before the sums.
+// the last stage.  W0 and the geometry come from the caller, which loads them before the barrier
+// that ends the flux phase so that their latency overlaps the wait.
 template <bool EXACT>
-__device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf &b, const double *sq,
-                                              const double *fs, int LC, int FC, int c0, int i) {
+__device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf &b, const double *fs, int c0, int i,
+                                              const double W0[5], const double4 &cg) {
     const int T = kTileCells;
     double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     unsigned short e[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) e[k] = k < a.max_contrib ? b.ct[k * T + i] : kNoContrib;
-    double W0[5];
-#pragma unroll
-    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
-    const double4 cg = b.cg[i];
     const Prim me = tile_prim(b.st, i);
 #pragma unroll
     for (int k = 0; k < 6; k++) {
@@ -838,7 +851,7 @@ __device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf 
             for (int q = 0; q < 5; q++) R[q] += fs[5 * j + q];
         }
     }
-    return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : sq[LC + i], R, W0, cg);
+    return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : rsqrt_nr(a.gamma * me.p * me.rho), R, W0, cg);
 }
 
 // Bounded wait on an mbarrier phase by every thread; on timeout the fault word is set.
@@ -851,7 +864,7 @@ __device__ __forceinline__ bool tile_wait(const StageArgs &a, uint64_t *bar, uin
 }
 
 // ---- one block per tile, all loads issued at the start (variant 2)
-// Shared memory: TileBuf (face fluxes over the records) | sq[2][LC] | mbarrier
+// Shared memory: TileBuf (face fluxes over the records) | mbarrier
 // The body is shared by tile_kernel (one solver) and tile_batch_kernel (several solvers in one
 // grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
 template <bool EXACT>
@@ -860,38 +873,50 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *
     const TileBuf b = tile_buf_at(smem_raw, LC, FC, MC);
     size_t off = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
     double *fs = reinterpret_cast<double *>(b.rec);
-    double *sq = reinterpret_cast<double *>(smem_raw + off);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
 
     const int c0 = tile * T;
     const int nloc = min(T, a.n_cells - c0);
-    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
-    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+    // Every load the copies depend on is issued before the first barrier, and none of them waits
+    // for another (the halo entries sit at a fixed stride per tile), so the copies start one
+    // memory latency after the block does.  The run's done flag is read alongside them.
+    const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+    const int i0 = threadIdx.x, i1 = threadIdx.x + T;
+    const int hx0 = i0 < a.halo_stride ? hrow[i0] : -1;
+    const int hx1 = i1 < a.halo_stride ? hrow[i1] : -1;
+    const int fp0 = a.tile_face_ptr[tile], fp1 = a.tile_face_ptr[tile + 1];
+    const long long rec_off = a.tile_rec_off[tile];
+    const bool done = !a.residual_only && a.ctl->done;
+    const int nf = fp1 - fp0;
 
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
-    if (threadIdx.x == 0) tile_issue_bulk(a, tile, b, bar);
-    for (int i = threadIdx.x; i < nh; i += kStageThreads) tile_gather_halo(a, b, nloc, i, a.tile_halo[h0 + i]);
+    if (done) return;  // uniform across the block (the run stopped: this stage leaves the state)
+    if (threadIdx.x == 0) tile_issue_bulk(a, tile, nf, rec_off, b, bar);
+    if (hx0 >= 0) tile_gather_halo(a, b, nloc, i0, hx0);
+    if (hx1 >= 0) tile_gather_halo(a, b, nloc, i1, hx1);
+    for (int i = threadIdx.x + 2 * T; i < a.halo_stride; i += T) {
+        const int h = hrow[i];
+        if (h >= 0) tile_gather_halo(a, b, nloc, i, h);
+    }
     cp_async_wait_all();
     if (!tile_wait(a, bar, 0)) {
         for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, 0); it++) {
         }  // let copies in flight land before the block leaves
         return;
     }
-    if (!EXACT) {
-        tile_roots<kStageThreads>(a, b, sq, LC, nloc + nh);
-        __syncthreads();
-    }
-    tile_fluxes<EXACT, kStageThreads>(a, b, sq, fs, LC, FC, nf, c0);
+    tile_fluxes<EXACT, kStageThreads>(a, b, fs, nf, c0);
+    double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
+    if ((int)threadIdx.x < nloc) tile_load_cell(a, c0, threadIdx.x, W0, cg);
     __syncthreads();
     double r2 = 0.0;
-    if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
+    if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, threadIdx.x, W0, cg);
     if (a.last_stage && !a.residual_only) block_sum_store(r2, partial);
 }
 
-template <bool EXACT, int MINB = 2>
+template <bool EXACT, int MINB>
 __global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     tile_body<EXACT>(a, blockIdx.x, a.partials + blockIdx.x, smem_raw);
 }
@@ -942,7 +967,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB) tile_batch_kernel(BatchSt
 // One block of kPipeThreads per SM walks tiles blockIdx.x, +gridDim.x, ...  While it evaluates
 // tile i from one buffer, the bulk copies and halo gathers of tile i+1 fill the other, so memory
 // traffic overlaps computation.  Halo indices are read into registers one tile ahead of their use.
-// Shared memory: TileBuf x 2 (face fluxes over each buffer's records) | sq[2][LC] | mbarrier x 2
+// Shared memory: TileBuf x 2 (face fluxes over each buffer's records) | mbarrier x 2
 constexpr int kPipeThreads = 512;
 
 template <bool EXACT>
@@ -957,12 +982,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         TileBuf r;
         r.st = k ? buf1.st : buf0.st;
         r.rec = k ? buf1.rec : buf0.rec;
-        r.cg = k ? buf1.cg : buf0.cg;
         r.ct = k ? buf1.ct : buf0.ct;
         return r;
     };
-    double *sq = reinterpret_cast<double *>(smem_raw + 2 * bb);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sq + 2 * LC);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + 2 * bb);
     const int G = gridDim.x;
     int tile = blockIdx.x;
     if (tile >= n_tiles) return;
@@ -974,11 +997,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
     __syncthreads();
     auto halo_index = [&](int t) {  // this thread's halo cell of tile t, or -1
         if (t >= n_tiles) return -1;
-        const int h0 = a.tile_halo_ptr[t], nh = a.tile_halo_ptr[t + 1] - h0;
-        return (int)threadIdx.x < nh ? a.tile_halo[h0 + threadIdx.x] : -1;
+        return (int)threadIdx.x < a.halo_stride ? a.tile_halo[(size_t)t * a.halo_stride + threadIdx.x] : -1;
+    };
+    auto issue = [&](int t, const TileBuf &tb, uint64_t *bar) {
+        tile_issue_bulk(a, t, a.tile_face_ptr[t + 1] - a.tile_face_ptr[t], a.tile_rec_off[t], tb, bar);
     };
     // prologue: tile 0 of this block in flight, halo indices of tile 1 on their way
-    if (threadIdx.x == 0) tile_issue_bulk(a, tile, buf0, &bars[0]);
+    if (threadIdx.x == 0) issue(tile, buf0, &bars[0]);
     {
         const int h = halo_index(tile);
         if (h >= 0) tile_gather_halo(a, buf0, min(T, a.n_cells - tile * T), threadIdx.x, h);
@@ -996,7 +1021,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
             if (threadIdx.x == 0) {
                 // the buffer was last read by ordinary loads; order those before the async-proxy writes
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tile_issue_bulk(a, next, nb, cur ? &bars[0] : &bars[1]);
+                issue(next, nb, cur ? &bars[0] : &bars[1]);
             }
             if (h_next >= 0) tile_gather_halo(a, nb, min(T, a.n_cells - next * T), threadIdx.x, h_next);
         }
@@ -1013,19 +1038,17 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         }
         const TileBuf b = pick(cur);
         const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-        const int nh = a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
         const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
-        if (!EXACT) {
-            tile_roots<kPipeThreads>(a, b, sq, LC, nloc + nh);
-            __syncthreads();
-        }
         double *fs = reinterpret_cast<double *>(b.rec);
-        tile_fluxes<EXACT, kPipeThreads>(a, b, sq, fs, LC, FC, nf, c0);
+        tile_fluxes<EXACT, kPipeThreads>(a, b, fs, nf, c0);
+        double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
+        if ((int)threadIdx.x < nloc) tile_load_cell(a, c0, threadIdx.x, W0, cg);
         __syncthreads();
         double r2 = 0.0;
-        if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, sq, fs, LC, FC, c0, threadIdx.x);
+        if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, threadIdx.x, W0, cg);
         if (a.last_stage && !a.residual_only) block_sum_store<kPipeThreads>(r2, a.partials + tile);
-        __syncthreads();  // buffer cur (with its fluxes) and sq are free again
+        __syncthreads();  // buffer cur (with its fluxes) is free again
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
@@ -1057,9 +1080,7 @@ __global__ void __launch_bounds__(kStageThreads) update_kernel(StageArgs a) {
 // Dynamic shared memory of tile_kernel (buffers = 1) and tile_pipe_kernel (buffers = 2).
 inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib, int buffers = 1) {
     const size_t bb = (tile_buf_bytes(smem_cells, smem_faces, max_contrib) + 15) & ~(size_t)15;
-    size_t b = buffers * bb + 2 * (size_t)smem_cells * 8;
-    b = (b + 15) & ~(size_t)15;
-    return b + 16;
+    return buffers * bb + 16;  // + one mbarrier per buffer
 }
 
 }  // namespace e3d

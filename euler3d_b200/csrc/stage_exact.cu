@@ -7,11 +7,11 @@ namespace e3d {
 
 // Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes) {
-    raise_smem_limit((const void *)tile_kernel<true>, smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<true, 4>, smem_bytes);
     if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<true>, pipe_smem_bytes);
 }
 
-void prepare_batch_exact(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<true, 2>, smem_bytes); }
+void prepare_batch_exact(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<true, 4>, smem_bytes); }
 
 // Update phase of a split stage (residual smoothing between residual and update).
 void launch_update_exact(const StageArgs &a, cudaStream_t s) {
@@ -20,11 +20,11 @@ void launch_update_exact(const StageArgs &a, cudaStream_t s) {
 
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_batch_kernel<true, 2><<<grid, kStageThreads, smem_bytes, s>>>(bs);
+    tile_batch_kernel<true, 4><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
-// variant 0: gather kernel, 1 block(s)/SM register budget; 1: gather kernel, 2 blocks/SM;
-// 2: face tiles, one block per tile; 3: face tiles, persistent and double-buffered
+// variant 0: gather kernel, registers for 2 blocks/SM; 1: gather kernel, 4 blocks/SM;
+// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and double-buffered
 void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
     if (variant == 3) {
@@ -32,11 +32,11 @@ void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant) {
         tile_pipe_kernel<true><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
-        tile_kernel<true><<<blocks, kStageThreads, smem, s>>>(a);
+        tile_kernel<true, 4><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 1) {
-        stage_kernel<true, 2><<<blocks, kStageThreads, 0, s>>>(a);
+        stage_kernel<true, 4><<<blocks, kStageThreads, 0, s>>>(a);
     } else {
-        stage_kernel<true, 1><<<blocks, kStageThreads, 0, s>>>(a);
+        stage_kernel<true, 2><<<blocks, kStageThreads, 0, s>>>(a);
     }
 }
 

@@ -5,7 +5,7 @@
 // cells, bulk copies of the tile's contiguous data plus cp.async gathers of its halo onto one
 // mbarrier, each face evaluated once, each cell summing its faces' F*S in ascending reference face
 // id (deterministic).  Cell records are 32 bytes (two float4), face records 24 bytes, so a tile's
-// staging is about half the double-precision one and three blocks fit on an SM.
+// staging is about half the double-precision one and six blocks fit on an SM.
 #pragma once
 #include "stage.cuh"
 
@@ -142,12 +142,20 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
     const int c0 = tile * T;
     const int nloc = min(T, a.n_cells - c0);
-    const int h0 = a.tile_halo_ptr[tile], nh = a.tile_halo_ptr[tile + 1] - h0;
-    const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+    // independent loads first, as in tile_body
+    const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+    const int i0 = threadIdx.x, i1 = threadIdx.x + T;
+    const int hx0 = i0 < a.halo_stride ? hrow[i0] : -1;
+    const int hx1 = i1 < a.halo_stride ? hrow[i1] : -1;
+    const int fp0 = a.tile_face_ptr[tile], fp1 = a.tile_face_ptr[tile + 1];
+    const long long rec_off = a.tile_rec32_off[tile];
+    const bool done = !a.residual_only && a.ctl->done;
+    const int nf = fp1 - fp0;
     const float gf = (float)a.gamma;
 
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
+    if (done) return;  // uniform across the block
     if (threadIdx.x == 0) {
         const uint32_t b_state = (uint32_t)nloc * 32u;
         const uint32_t b_rec = round16(24u * (uint32_t)nf);
@@ -156,15 +164,20 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
         const uint32_t b_ct = (uint32_t)MC * T * 2u;
         mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
         bulk_g2s(st, a.q32in + 2 * (size_t)c0, b_state, bar);
-        bulk_g2s(rec, a.tile_rec32 + a.tile_rec32_off[tile], b_rec, bar);
+        bulk_g2s(rec, a.tile_rec32 + rec_off, b_rec, bar);
         for (int k = 0; k < 5; k++) bulk_g2s(w0s + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
         bulk_g2s(cgs, a.cgeo32 + c0, b_cg, bar);
         bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
     }
-    for (int i = threadIdx.x; i < nh; i += kStageThreads) {
-        const int h = a.tile_halo[h0 + i];
+    auto gather = [&](int i, int h) {
         cp_async16(st + 2 * (nloc + i), a.q32in + 2 * (size_t)h);
         cp_async16(st + 2 * (nloc + i) + 1, a.q32in + 2 * (size_t)h + 1);
+    };
+    if (hx0 >= 0) gather(i0, hx0);
+    if (hx1 >= 0) gather(i1, hx1);
+    for (int i = threadIdx.x + 2 * T; i < a.halo_stride; i += T) {
+        const int h = hrow[i];
+        if (h >= 0) gather(i, h);
     }
     cp_async_wait_all();
     if (!tile_wait(a, bar, 0)) {
@@ -256,7 +269,6 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
 
 template <int MINB>
 __global__ void __launch_bounds__(kStageThreads, MINB) tile_kernel_f32(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     tile_body_f32(a, blockIdx.x, a.partials + blockIdx.x, smem_raw);
 }

@@ -1,4 +1,5 @@
-// FP64 instantiations of the stage kernels: restructured arithmetic, FMA contraction allowed.
+// FP64 instantiations of the stage kernels: restructured arithmetic, fused multiply-adds where the
+// source writes fma() (built with -fmad=false, so nothing else is contracted).
 #include "common.hpp"
 #include "stage.cuh"
 
@@ -6,12 +7,12 @@ namespace e3d {
 
 // Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
-    raise_smem_limit((const void *)tile_kernel<false>, smem_bytes);
-    raise_smem_limit((const void *)tile_kernel<false, 3>, smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<false, 4>, smem_bytes);
+    raise_smem_limit((const void *)tile_kernel<false, 7>, smem_bytes);
     if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<false>, pipe_smem_bytes);
 }
 
-void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false, 2>, smem_bytes); }
+void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false, 6>, smem_bytes); }
 
 // Update phase of a split stage (residual smoothing between residual and update).
 void launch_update_fast(const StageArgs &a, cudaStream_t s) {
@@ -20,27 +21,27 @@ void launch_update_fast(const StageArgs &a, cudaStream_t s) {
 
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_batch_kernel<false, 2><<<grid, kStageThreads, smem_bytes, s>>>(bs);
+    tile_batch_kernel<false, 6><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
-// variant 0: gather kernel, 2 block(s)/SM register budget; 1: gather kernel, 3 blocks/SM;
-// 2: face tiles, one block per tile; 3: face tiles, persistent and double-buffered; 4: face tiles
-// with a three-blocks-per-SM register budget
+// variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;
+// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and double-buffered;
+// 4: face tiles with registers for 7 blocks/SM
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
     if (variant == 4) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
-        tile_kernel<false, 3><<<blocks, kStageThreads, smem, s>>>(a);
+        tile_kernel<false, 7><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 3) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, 2);
         tile_pipe_kernel<false><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
-        tile_kernel<false><<<blocks, kStageThreads, smem, s>>>(a);
+        tile_kernel<false, 4><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 1) {
-        stage_kernel<false, 3><<<blocks, kStageThreads, 0, s>>>(a);
+        stage_kernel<false, 5><<<blocks, kStageThreads, 0, s>>>(a);
     } else {
-        stage_kernel<false, 2><<<blocks, kStageThreads, 0, s>>>(a);
+        stage_kernel<false, 4><<<blocks, kStageThreads, 0, s>>>(a);
     }
 }
 

@@ -245,7 +245,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *params, e3d_
  * allocator may not be called.  e3d_solver_run itself may allocate (its history buffer grows with
  * max_iter and it instantiates CUDA graphs); this call allocates nothing.  It computes the same
  * iterations with the same kernels, launched directly, and keeps its scratch (the per-block RMS
- * partial sums and the RMS history) in one 1 MiB file-scope device array that every device loading
+ * partial sums and the RMS history) in one 1.5 MiB file-scope device array that every device loading
  * the library holds until the process exits.  Limits: at most 16,777,216 cells and 65,536
  * iterations per call; larger requests fail with E3D_ERR_INVALID_ARG.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress), so make that first call before any
