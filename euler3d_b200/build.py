@@ -1,7 +1,7 @@
 """Build recipe of the euler3d_b200 shared library (sm_100a) with nvcc, in-tree.
 
 ``python -m euler3d_b200.build`` (or ``build()``) compiles ``csrc/*`` into
-``euler3d_b200/libeuler3d_b200.so``.  The double-precision translation units are compiled
+``euler3d_b200/libeuler3d_b200.so``.  The CUDA translation units are compiled
 with ``-fmad=false`` so that no multiply-add is contracted behind the source's back: the exact
 mode rounds as the reference's source order does, and the FP64 mode fuses only where its source
 says ``fma()``, so every kernel variant computes the same bits whatever its register budget.  Host
@@ -29,7 +29,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 SOURCES = [
     ("stage_exact.cu", ["-fmad=false"]),
     ("stage_fast.cu", ["-fmad=false"]),
-    ("stage_f32.cu", ["-fmad=true"]),
+    ("stage_f32.cu", ["-fmad=false"]),
     ("solver.cu", ["-fmad=false"]),
     ("batch.cu", ["-fmad=false"]),
     ("outputs.cu", ["-fmad=false"]),

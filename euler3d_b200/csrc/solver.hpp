@@ -322,7 +322,7 @@ struct Solver {
         ghost_copy.release();
     }
 
-    // Without tuning: the face-tile kernel (seven blocks per SM in FP64, six in FP32_FLUX), or the
+    // Without tuning: the face-tile kernel (seven blocks per SM in FP64, eight in FP32_FLUX), or the
     // gather kernel when the mesh does not fit the tiles.
     void use_default_variant() {
         for (auto &m : variant_ms) m = -1.0f;

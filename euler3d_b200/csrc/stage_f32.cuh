@@ -5,7 +5,7 @@
 // cells, bulk copies of the tile's contiguous data plus cp.async gathers of its halo onto one
 // mbarrier, each face evaluated once, each cell summing its faces' F*S in ascending reference face
 // id (deterministic).  Cell records are 32 bytes (two float4), face records 24 bytes, so a tile's
-// staging is about half the double-precision one and six blocks fit on an SM.
+// staging is about half the double-precision one and eight blocks fit on an SM.
 #pragma once
 #include "stage.cuh"
 
@@ -36,50 +36,53 @@ __device__ __forceinline__ void make_rec32(float4 *dst, double rho, double u, do
 }
 
 // Roe flux with Harten's fix (Solver::Roe, src/solver/ConvectiveFluxesSchemes.cpp:10-165) in single
-// precision, written as F = (F_L + F_R - sum_k a_k r_k) / 2 like roe_fast.
+// precision, written as F = (F_L + F_R - sum_k a_k r_k) / 2 like roe_fast.  Built without
+// multiply-add contraction: it fuses where the source writes fmaf(), so the rounding is fixed by
+// the source in every kernel variant.
 __device__ __forceinline__ void roe_f32(const PrimF &L, const PrimF &R, float nx, float ny, float nz, float g,
                                         float F[5]) {
     const float inv = rcp_f(L.s + R.s);
     const float wl = L.s * inv, wr = R.s * inv;
-    const float ut = L.u * wl + R.u * wr, vt = L.v * wl + R.v * wr, wt = L.w * wl + R.w * wr;
-    const float ht = L.H * wl + R.H * wr;
+    const float ut = fmaf(L.u, wl, R.u * wr), vt = fmaf(L.v, wl, R.v * wr), wt = fmaf(L.w, wl, R.w * wr);
+    const float ht = fmaf(L.H, wl, R.H * wr);
     const float rt = L.s * R.s;
-    const float q2t = ut * ut + vt * vt + wt * wt;
-    const float c2 = (g - 1.0f) * (ht - 0.5f * q2t);
+    const float q2t = fmaf(ut, ut, fmaf(vt, vt, wt * wt));
+    const float c2 = (g - 1.0f) * fmaf(-0.5f, q2t, ht);
     const float rc = rsqrt_f(c2);
     const float ct = c2 * rc, ic2 = rc * rc;
-    const float Vt = ut * nx + vt * ny + wt * nz;
-    const float Vl = L.u * nx + L.v * ny + L.w * nz;
-    const float Vr = R.u * nx + R.v * ny + R.w * nz;
+    const float Vt = fmaf(ut, nx, fmaf(vt, ny, wt * nz));
+    const float Vl = fmaf(L.u, nx, fmaf(L.v, ny, L.w * nz));
+    const float Vr = fmaf(R.u, nx, fmaf(R.v, ny, R.w * nz));
     const float drho = R.rho - L.rho, dp = R.p - L.p, dV = Vr - Vl;
     const float du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
     const float delta = (1.0f / 15.0f) * (g * L.p * L.r);
     float lam1 = fabsf(Vt - ct), lam5 = fabsf(Vt + ct);
     if (!(lam1 > delta) || !(lam5 > delta)) {
         const float h = 7.5f * (L.rho * L.r);
-        if (!(lam1 > delta)) lam1 = (lam1 * lam1 + delta * delta) * h;
-        if (!(lam5 > delta)) lam5 = (lam5 * lam5 + delta * delta) * h;
+        if (!(lam1 > delta)) lam1 = fmaf(lam1, lam1, delta * delta) * h;
+        if (!(lam5 > delta)) lam5 = fmaf(lam5, lam5, delta * delta) * h;
     }
     const float rcdv = rt * ct * dV;
     const float a1 = 0.5f * lam1 * (dp - rcdv) * ic2;
     const float a5 = 0.5f * lam5 * (dp + rcdv) * ic2;
     const float aV = fabsf(Vt);
-    const float a2 = aV * (drho - dp * ic2);
+    const float a2 = aV * fmaf(-dp, ic2, drho);
     const float a3 = aV * rt;
     const float a15 = a1 + a5, d51 = (a5 - a1) * ct, asum = a15 + a2;
     const float mL = L.rho * Vl, mR = R.rho * Vr, ps = L.p + R.p;
     F[0] = 0.5f * (mL + mR - asum);
-    F[1] = 0.5f * (mL * L.u + mR * R.u + ps * nx - (asum * ut + d51 * nx + a3 * (du - dV * nx)));
-    F[2] = 0.5f * (mL * L.v + mR * R.v + ps * ny - (asum * vt + d51 * ny + a3 * (dv - dV * ny)));
-    F[3] = 0.5f * (mL * L.w + mR * R.w + ps * nz - (asum * wt + d51 * nz + a3 * (dw - dV * nz)));
-    F[4] = 0.5f * (mL * L.H + mR * R.H - (a15 * ht + d51 * Vt + a2 * (0.5f * q2t) + a3 * (ut * du + vt * dv + wt * dw - Vt * dV)));
+    F[1] = 0.5f * (fmaf(mL, L.u, fmaf(mR, R.u, ps * nx)) - fmaf(asum, ut, fmaf(d51, nx, a3 * fmaf(-dV, nx, du))));
+    F[2] = 0.5f * (fmaf(mL, L.v, fmaf(mR, R.v, ps * ny)) - fmaf(asum, vt, fmaf(d51, ny, a3 * fmaf(-dV, ny, dv))));
+    F[3] = 0.5f * (fmaf(mL, L.w, fmaf(mR, R.w, ps * nz)) - fmaf(asum, wt, fmaf(d51, nz, a3 * fmaf(-dV, nz, dw))));
+    F[4] = 0.5f * (fmaf(mL, L.H, mR * R.H) -
+                   fmaf(a15, ht, fmaf(d51, Vt, fmaf(a2, 0.5f * q2t, a3 * fmaf(-Vt, dV, fmaf(ut, du, fmaf(vt, dv, wt * dw)))))));
 }
 
 // AUSM (Liou & Steffen 1993) in single precision; c = gamma p r, M = V rho r.
 __device__ __forceinline__ void ausm_f32(const PrimF &L, const PrimF &R, float nx, float ny, float nz, float g,
                                          float F[5]) {
     const float cl = g * L.p * L.r, cr = g * R.p * R.r;
-    const float Vl = L.u * nx + L.v * ny + L.w * nz, Vr = R.u * nx + R.v * ny + R.w * nz;
+    const float Vl = fmaf(L.u, nx, fmaf(L.v, ny, L.w * nz)), Vr = fmaf(R.u, nx, fmaf(R.v, ny, R.w * nz));
     const float Ml = Vl * (L.rho * L.r), Mr = Vr * (R.rho * R.r);
     float mp, pp, mm, pm;
     if (fabsf(Ml) <= 1.0f) {
@@ -96,13 +99,13 @@ __device__ __forceinline__ void ausm_f32(const PrimF &L, const PrimF &R, float n
         mm = 0.5f * (Mr - fabsf(Mr));
         pm = Mr < 0.0f ? 1.0f : 0.0f;
     }
-    const float mi = mp + mm, pi = pp * L.p + pm * R.p;
+    const float mi = mp + mm, pi = fmaf(pp, L.p, pm * R.p);
     const float al = fmaxf(mi, 0.0f) * (L.rho * cl), ar = fminf(mi, 0.0f) * (R.rho * cr);
     F[0] = al + ar;
-    F[1] = al * L.u + ar * R.u + pi * nx;
-    F[2] = al * L.v + ar * R.v + pi * ny;
-    F[3] = al * L.w + ar * R.w + pi * nz;
-    F[4] = al * L.H + ar * R.H;
+    F[1] = fmaf(al, L.u, fmaf(ar, R.u, pi * nx));
+    F[2] = fmaf(al, L.v, fmaf(ar, R.v, pi * ny));
+    F[3] = fmaf(al, L.w, fmaf(ar, R.w, pi * nz));
+    F[4] = fmaf(al, L.H, ar * R.H);
 }
 
 __device__ __forceinline__ PrimF prim32(const float4 *st, int i) {
@@ -110,13 +113,13 @@ __device__ __forceinline__ PrimF prim32(const float4 *st, int i) {
     return PrimF{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 }
 
-// Shared memory: st[LC] 32-byte records | rec[FC] | w0[5][T] (double) | cg[T] | ct[MC][T] | mbarrier.
-// The five float F*S of face j are written over its 24-byte record (fs[6 j + k]), which only the
-// thread evaluating the face reads.
-// | mbarrier
+// Shared memory: st[LC] 32-byte records | rec[FC] | ct[MC][T] | mbarrier.  The five float F*S of
+// face j are written over its 24-byte record (fs[6 j + k]), which only the thread evaluating the
+// face reads.  W0 and the cell geometry stay in global memory (prefetched into L2 when the tile
+// starts, read into registers before the flux phase ends), as in tile_body.
 inline size_t tile32_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
-    size_t b = (size_t)smem_cells * 32 + ((24u * (size_t)smem_faces + 15) & ~(size_t)15) + 5 * kTileCells * 8 +
-               kTileCells * 16 + (size_t)max_contrib * kTileCells * 2;
+    size_t b = (size_t)smem_cells * 32 + ((24u * (size_t)smem_faces + 15) & ~(size_t)15) +
+               (size_t)max_contrib * kTileCells * 2;
     b = (b + 15) & ~(size_t)15;
     return b + 16;
 }
@@ -130,10 +133,6 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
     off += (size_t)LC * 32;
     FaceRec32 *rec = reinterpret_cast<FaceRec32 *>(smem_raw + off);
     off += round16(24u * FC);
-    double *w0s = reinterpret_cast<double *>(smem_raw + off);
-    off += 5 * T * 8;
-    float4 *cgs = reinterpret_cast<float4 *>(smem_raw + off);
-    off += T * 16;
     unsigned short *cts = reinterpret_cast<unsigned short *>(smem_raw + off);
     off += (size_t)MC * T * 2;
     off = (off + 15) & ~(size_t)15;
@@ -162,12 +161,12 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
         const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
         const uint32_t b_cg = (uint32_t)nloc * 16u;
         const uint32_t b_ct = (uint32_t)MC * T * 2u;
-        mbar_expect_tx(bar, b_state + b_rec + 5u * b_w0 + b_cg + b_ct);
+        mbar_expect_tx(bar, b_state + b_rec + b_ct);
         bulk_g2s(st, a.q32in + 2 * (size_t)c0, b_state, bar);
         bulk_g2s(rec, a.tile_rec32 + rec_off, b_rec, bar);
-        for (int k = 0; k < 5; k++) bulk_g2s(w0s + k * T, a.w0 + (size_t)k * a.w0_stride + c0, b_w0, bar);
-        bulk_g2s(cgs, a.cgeo32 + c0, b_cg, bar);
         bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+        for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
+        bulk_prefetch_l2(a.cgeo32 + c0, b_cg);
     }
     auto gather = [&](int i, int h) {
         cp_async16(st + 2 * (nloc + i), a.q32in + 2 * (size_t)h);
@@ -216,10 +215,17 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
 #pragma unroll
         for (int k = 0; k < 5; k++) fs[6 * j + k] = F[k] * fr.S;
     }
+    const int i = threadIdx.x;
+    double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    float4 cg = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i < nloc) {  // the owner's W0 and geometry: their latency overlaps the barrier's wait
+#pragma unroll
+        for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
+        cg = a.cgeo32[c0 + i];
+    }
     __syncthreads();
 
     double r2 = 0.0;
-    const int i = threadIdx.x;
     if (i < nloc) {
         const PrimF me = prim32(st, i);
         double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -235,9 +241,8 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
             for (int q = 0; q < 5; q++) R[q] += sg * (double)fs[6 * j + q];
         }
         // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
-        const float4 cg = cgs[i];
         const float snd = gf * me.p * me.r;
-        const float lam = 0.5f * ((fabsf(me.u) + snd) * cg.x + (fabsf(me.v) + snd) * cg.y + (fabsf(me.w) + snd) * cg.z);
+        const float lam = 0.5f * fmaf(fabsf(me.u) + snd, cg.x, fmaf(fabsf(me.v) + snd, cg.y, (fabsf(me.w) + snd) * cg.z));
         const int c = c0 + i;
         if (a.residual_only) {
             const int o = a.new2old[c];
@@ -246,13 +251,13 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
             a.dt_out[o] = (double)(a.cfl * cg.w / lam);
         } else {
             // W = W0 - alpha dt R / V in double (alpha dt / V = alpha cfl / lambda)
-            const double coef = a.alpha * a.cfl / (double)lam;
+            const double coef = a.alpha * a.cfl * rcp_nr((double)lam);
             double W[5];
 #pragma unroll
-            for (int k = 0; k < 5; k++) W[k] = w0s[k * T + i] - coef * R[k];
-            const double ir = 1.0 / W[0];
+            for (int k = 0; k < 5; k++) W[k] = fma(-coef, R[k], W0[k]);
+            const double ir = rcp_nr(W[0]);
             const double u = W[1] * ir, v = W[2] * ir, w = W[3] * ir;
-            const double p = (a.gamma - 1.0) * (W[4] - 0.5 * (W[1] * u + W[2] * v + W[3] * w));
+            const double p = (a.gamma - 1.0) * fma(-0.5, fma(W[1], u, fma(W[2], v, W[3] * w)), W[4]);
             const double H = (W[4] + p) * ir;
             make_rec32(a.q32out + 2 * (size_t)c, W[0], u, v, w, p, H, a.gamma);
             if (a.last_stage) {  // the conservative state carries over exactly in double
