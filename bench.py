@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="hexahedra per box edge (6 tets each)")
     ap.add_argument("--precision", choices=["fp64", "fp64_exact", "fp32"], default="fp64")
     ap.add_argument("--ordering", choices=["spatial", "rcm", "native"], default="spatial")
-    ap.add_argument("--kernel", type=int, default=0, help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined face tiles")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined face tiles, 5 face tiles at 7 blocks/SM "
+                         "(FP32_FLUX: 3 and 4 are its two face-tile register budgets)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--mode", choices=["all", "stage", "served"], default="all",

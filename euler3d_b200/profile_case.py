@@ -15,7 +15,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64, help="hexahedra per box edge (6 tetrahedra each)")
     ap.add_argument("--kernel", type=int, default=0, help="0 autotuned, 1/2 gather, 3 face tiles, 4 pipelined tiles, "
-                                                               "5 face tiles at 3 blocks/SM")
+                                                               "5 face tiles at 7 blocks/SM")
     ap.add_argument("--precision", choices=["fp64", "fp64_exact", "fp32"], default="fp64")
     ap.add_argument("--iters", type=int, default=2)
     args = ap.parse_args()

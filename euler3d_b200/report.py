@@ -7,6 +7,10 @@
                                       # residual drop at checkpoints, the FP32 fields and lift / drag
                                       # against FP64 after the same iterations, and where the FP32
                                       # residual stalls
+  python -m euler3d_b200.report c4    # 256 uneven instances (bump channels and biconvex O-grids of
+                                      # 5k-200k cells, Mach 0.3-0.85, AoA -4..6, Roe/AUSM) run as
+                                      # one batch to a 1e-8 drop, FP32_FLUX then FP64, against the
+                                      # plain one-at-a-time FP64 path on a sample of them
 
 Meshes are generated in-process (synthetic, seeded).  The FP64 solution stands for the oracle at
 this size: the FP64 path equals the CPU restatement to 1e-10 per cell on the small cases the tests
@@ -22,6 +26,7 @@ import numpy as np
 
 from . import _lib
 from . import meshgen as mg
+from . import serve
 from .solver import EulerSolver, FlowConfig, Mesh
 
 
@@ -83,9 +88,41 @@ def c2(max_iter=200_000):
     return out
 
 
+def c4(n=256, max_iter=20_000, plain_sample=32):
+    """n instances drawn with seed 3 (bump channels and biconvex O-grids, cells log-uniform in
+    [5k, 200k], Mach uniform in [0.3, 0.85], AoA in [-4, 6] degrees, Roe or AUSM), all present at
+    the start, each to a 1e-8 density-residual drop (at most max_iter iterations).  They run as one
+    batch with the precision ladder: FP32_FLUX until a solve's residual stalls, then FP64 from that
+    state.  Beside it the plain FP64 path solves the first plain_sample instances one at a time;
+    its solves/s on that sample stands for the whole set (solving all of them one at a time would
+    take several minutes more), and its lift and drag are compared with the batch's.  Wall-clock
+    spans include the host mesh preparation (four threads) in both."""
+    reqs = serve.request_stream(n, 0.0, cells=(5000, 200_000), seed=3, drops=(1e-8,),
+                                schemes=(_lib.SCHEME_ROE, _lib.SCHEME_AUSM))
+    srv = serve.Server(max_members=n, ladder=True, max_iter=max_iter)
+    served = srv.serve(reqs)
+    row = {"config": "c4", "instances": n, "cells_total": int(sum(r.cells for r in served)), "max_iter": max_iter,
+           "batch_ladder": serve.summarize(served), "peak_members": srv.peak_members,
+           "peak_device_bytes": srv.peak_bytes, "device_busy_s": srv.step_ms / 1e3,
+           "fp32_iteration_share": (sum(r.fp32_iterations for r in served) /
+                                    max(sum(max(r.iterations, 0) for r in served), 1))}
+    b = row["batch_ladder"]
+    b["cell_stage_updates_per_s"] = 5.0 * b["cell_iterations"] / b["seconds"]
+    sample = [q for q in reqs if q.rid < plain_sample]
+    base = serve.serve_plain(sample, max_iter=max_iter)
+    p = serve.summarize(base)
+    p["cell_stage_updates_per_s"] = 5.0 * p["cell_iterations"] / p["seconds"]
+    row["plain_sample"] = p
+    row["plain_sample_size"] = len(sample)
+    d = serve._diffs(base, [r for r in served if r.rid < plain_sample])
+    row["sample_diffs"] = {k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "same_outcome")}
+    row["speedup_solves_per_s"] = b["solves_per_s"] / p["solves_per_s"]
+    return [row]
+
+
 def main(argv=None):
     which = (argv or sys.argv[1:] or ["c1"])[0]
-    rows = {"c1": c1, "c2": c2}[which]()
+    rows = {"c1": c1, "c2": c2, "c4": c4}[which]()
     for r in rows:
         print(json.dumps(r), flush=True)
 
