@@ -266,7 +266,7 @@ struct Solver {
     float variant_ms[kStageVariants] = {};
 
     // Variants compiled for this precision and possible on this mesh.  FP32_FLUX mode has face-tile
-    // kernels only (variants 2 and 3 are its two register budgets); the three-blocks-per-SM face-tile
+    // kernels only (variants 2 and 3 are its two register budgets); the seven-blocks-per-SM face-tile
     // kernel exists for FP64 only (in FP64_EXACT it would spill).
     bool variant_ok(int v) const {
         if (v < 0 || v >= kStageVariants) return false;

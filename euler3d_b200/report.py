@@ -115,7 +115,8 @@ def c4(n=256, max_iter=20_000, plain_sample=32):
     row["plain_sample"] = p
     row["plain_sample_size"] = len(sample)
     d = serve._diffs(base, [r for r in served if r.rid < plain_sample])
-    row["sample_diffs"] = {k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "same_outcome")}
+    row["sample_diffs"] = {k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "converged_max_rel_diff_cl",
+                                             "converged_max_rel_diff_cd", "same_outcome")}
     row["speedup_solves_per_s"] = b["solves_per_s"] / p["solves_per_s"]
     return [row]
 

@@ -359,13 +359,21 @@ def serve_plain(requests: Sequence[SolveRequest], device: int = 0, precision: in
 
 
 def _diffs(base: Sequence[SolveResult], other: Sequence[SolveResult]) -> Dict[str, object]:
+    """Lift and drag differences between two runs of the same requests: over every solve that ended
+    without error in both, and over those that reached their tolerance in both (a solve stopped at
+    max_iter is unconverged, and two paths to the same iteration count need not agree there)."""
     by = {r.rid: r for r in other}
     ok = [b for b in base if b.status == _lib.E3D_OK and by[b.rid].status == _lib.E3D_OK]
+    conv = [b for b in ok if b.stop_reason == _lib.STOP_RESIDUAL and by[b.rid].stop_reason == _lib.STOP_RESIDUAL]
+
     # relative to the coefficient's size, at least 1e-2 (a near-zero lift has no relative error)
-    dl = [abs(b.cl - by[b.rid].cl) / max(abs(b.cl), 1e-2) for b in ok]
-    dd = [abs(b.cd - by[b.rid].cd) / max(abs(b.cd), 1e-2) for b in ok]
+    def rel(rs, key):
+        d = [abs(getattr(b, key) - getattr(by[b.rid], key)) / max(abs(getattr(b, key)), 1e-2) for b in rs]
+        return max(d) if d else None
+
     mism = [b for b in base if (b.status, b.stop_reason) != (by[b.rid].status, by[b.rid].stop_reason)]
-    return {"max_rel_diff_cl": max(dl) if dl else None, "max_rel_diff_cd": max(dd) if dd else None,
+    return {"max_rel_diff_cl": rel(ok, "cl"), "max_rel_diff_cd": rel(ok, "cd"),
+            "converged_max_rel_diff_cl": rel(conv, "cl"), "converged_max_rel_diff_cd": rel(conv, "cd"),
             "same_outcome": not mism,
             "outcome_mismatches": [{"rid": b.rid, "cells": b.cells, "plain": [b.status, b.stop_reason, b.iterations],
                                     "served": [by[b.rid].status, by[b.rid].stop_reason, by[b.rid].iterations]}
@@ -404,7 +412,8 @@ def compare(requests: Sequence[SolveRequest], precision: int = _lib.PREC_FP64, i
         out["speedup_solves_per_s"] = out["served"]["solves_per_s"] / out["plain"]["solves_per_s"]
         if lad is not None:
             d = _diffs(base, lad)
-            out["served_ladder"].update({k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "same_outcome")})
+            out["served_ladder"].update({k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "converged_max_rel_diff_cl",
+                                                           "converged_max_rel_diff_cd", "same_outcome")})
             out["served_ladder"]["speedup_solves_per_s"] = (out["served_ladder"]["solves_per_s"] /
                                                             out["plain"]["solves_per_s"])
     return out

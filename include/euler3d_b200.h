@@ -210,7 +210,7 @@ typedef struct e3d_run_params {
 	                                     events (stats.stage_ms); 0: CUDA graphs */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
 	                                     register budgets; 3: face tiles; 4: persistent double-buffered
-	                                     face tiles; 5: face tiles at three blocks per SM (FP64 only)
+	                                     face tiles; 5: face tiles at seven blocks per SM (FP64 only)
 	                                     (kept for later runs) */
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
