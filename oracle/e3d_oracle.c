@@ -379,8 +379,8 @@ static void smooth_pass(const orc_mesh *m, const double *orig, const double *las
 
 long long orc_smooth_residuals(const orc_mesh *m, double *R) {
 	const size_t n5 = 5 * (size_t) m->n_cells;
-	double *orig = (double *) malloc(sizeof(double) * (n5 ? n5 : 1));
-	double *last = (double *) malloc(sizeof(double) * (n5 ? n5 : 1));
+	double *orig = (double *) calloc(n5 ? n5 : 1, sizeof(double));
+	double *last = (double *) calloc(n5 ? n5 : 1, sizeof(double));
 	if (!orig || !last) {
 		free(orig);
 		free(last);
