@@ -1020,11 +1020,18 @@ void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s) {
     if (rp->sampling <= 0) throw Error(E3D_ERR_INVALID_ARG, "sampling must be a positive integer");
     if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
     const int max_iter = std::max(rp->max_iter, 0);
+    // The history and sample buffers grow geometrically from a floor, so that a short run (a
+    // warm-up, a first chunk) leaves room for the next one: a reallocation also throws away the
+    // instantiated graph, whose finalize and coefficient kernels hold these pointers.
+    auto grown = [](int need, int cap, int floor_) {
+        return (int)std::min<int64_t>(INT32_MAX, std::max<int64_t>({need, 2 * (int64_t)cap, floor_}));
+    };
     if (S->hist_cap < max_iter || !S->hist.p) {
         E3D_CUDA(cudaStreamSynchronize(s));
+        const int cap = grown(max_iter, S->hist_cap, 1024);
         S->hist.release();
-        S->hist.alloc(std::max(max_iter, 1));
-        S->hist_cap = std::max(max_iter, 1);
+        S->hist.alloc(cap);
+        S->hist_cap = cap;
         if (S->graph) {  // the captured finalize kernels hold the old history pointer
             cudaGraphExecDestroy(S->graph);
             S->graph = nullptr;
@@ -1034,9 +1041,10 @@ void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s) {
     const int need = max_iter / rp->sampling + 1;
     if (S->sample_cap < need || !S->samples.p) {
         E3D_CUDA(cudaStreamSynchronize(s));
+        const int cap = grown(need, S->sample_cap, 256);
         S->samples.release();
-        S->samples.alloc(7 * (size_t)need);
-        S->sample_cap = need;
+        S->samples.alloc(7 * (size_t)cap);
+        S->sample_cap = cap;
         if (S->graph) {  // the captured coefficient kernels hold the old pointer
             cudaGraphExecDestroy(S->graph);
             S->graph = nullptr;
@@ -1222,18 +1230,34 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
         int64_t launches = 0;
         double stage_ms = 0.0;
         int64_t stage_launches = 0;
-        if (!rp->profile_stages) {
+        if (rp->profile_stages < 0 || rp->profile_stages > 2) throw Error(E3D_ERR_INVALID_ARG, "profile_stages must be 0, 1 or 2");
+        if (rp->profile_stages != 1) {
             int every = rp->check_every > 0 ? rp->check_every : 32;
             every += every & 1;  // whole graphs start and end on buffer 0
-            S->build_graph(every);
+            const bool timed = rp->profile_stages == 2;
+            S->build_graph(every, timed);
             E3D_CUDA(cudaEventRecord(S->ev0, S->stream));
             int launched_iters = 0;
+            int n_before = 0;  // iterations done before this graph launch (the control block's RMS count)
             while (max_iter > 0) {
                 E3D_CUDA(cudaGraphLaunch(S->graph, S->stream));
                 launches += (int64_t)S->kernels_per_iteration() * every;
                 launched_iters += every;
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
                 E3D_CUDA(cudaStreamSynchronize(S->stream));
+                if (timed) {  // the stage kernels of the iterations that ran (later ones return at once)
+                    const int ran = std::min(every, S->ctl_host->n_rms - n_before);
+                    const int ns = S->n_stages();
+                    for (int i = 0; i < ran; i++)
+                        for (int st_i = 0; st_i < ns; st_i++) {
+                            const cudaEvent_t *e = S->graph_ev.data() + 2 * ((size_t)ns * i + st_i);
+                            float ems = 0.f;
+                            E3D_CUDA(cudaEventElapsedTime(&ems, e[0], e[1]));
+                            stage_ms += ems;
+                        }
+                    stage_launches += (int64_t)ran * ns;
+                    n_before = S->ctl_host->n_rms;
+                }
                 if (S->ctl_host->done) break;
                 if (launched_iters > max_iter + every)
                     throw Error(E3D_ERR_TIMEOUT, "run did not reach its stop condition");

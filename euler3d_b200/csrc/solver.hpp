@@ -160,6 +160,8 @@ struct Solver {
 
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
+    bool graph_timed = false;             // the graph records graph_ev around its stage kernels
+    std::vector<cudaEvent_t> graph_ev;    // [iteration][stage][begin, end] of a timed graph
     Batch *batch = nullptr;        // the batch running this solver, if any (batch.cu)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t prof_ev[10] = {};
@@ -170,6 +172,7 @@ struct Solver {
         if (ev1) cudaEventDestroy(ev1);
         for (auto e : prof_ev)
             if (e) cudaEventDestroy(e);
+        for (auto e : graph_ev) cudaEventDestroy(e);
         DevBuf<int> *ib[] = {&cptr, &new2old_d, &ghost_ref_d, &wall_cell, &tile_halo_ptr, &tile_halo, &tile_face_ptr};
         for (auto *b : ib) b->release();
         tile_rec.release();
@@ -411,11 +414,14 @@ struct Solver {
     }
 
     // One iteration of EulerSolver::Run (src/solver/EulerSolver.cpp:84-153) starting from q[in_buf];
-    // returns the kernels launched.
-    int enqueue_iteration(int in_buf) {
+    // returns the kernels launched.  With ev, event pair ev[2 s], ev[2 s + 1] brackets stage s (as
+    // external event-record nodes when the stream is being captured).
+    int enqueue_iteration(int in_buf, const cudaEvent_t *ev = nullptr) {
         int b = in_buf;
         for (int s = 0; s < n_stages(); s++) {
+            if (ev) E3D_CUDA(cudaEventRecordWithFlags(ev[2 * s], stream, cudaEventRecordExternal));
             enqueue_stage(b, s, partials.p);
+            if (ev) E3D_CUDA(cudaEventRecordWithFlags(ev[2 * s + 1], stream, cudaEventRecordExternal));
             b = 1 - b;
         }
         launch_finalize(finalize_args(partials.p, hist.p), stream);
@@ -423,17 +429,25 @@ struct Solver {
         return kernels_per_iteration();
     }
 
-    void build_graph(int iters) {
-        if (graph && graph_iters == iters) return;
+    // A graph of `iters` iterations; with `timed`, an event pair around every stage kernel (see
+    // e3d_run_params.profile_stages = 2).
+    void build_graph(int iters, bool timed = false) {
+        if (graph && graph_iters == iters && graph_timed == timed) return;
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
+        }
+        const size_t n_ev = timed ? 2 * (size_t)n_stages() * iters : 0;
+        while (graph_ev.size() < n_ev) {
+            cudaEvent_t e;
+            E3D_CUDA(cudaEventCreate(&e));
+            graph_ev.push_back(e);
         }
         cudaGraph_t g;
         E3D_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         int b = 0;
         for (int i = 0; i < iters; i++) {
-            enqueue_iteration(b);
+            enqueue_iteration(b, timed ? graph_ev.data() + 2 * (size_t)n_stages() * i : nullptr);
             b = 1 - b;  // five stages flip the buffer once per iteration
         }
         cudaError_t cap = cudaStreamEndCapture(stream, &g);
@@ -442,6 +456,7 @@ struct Solver {
         cudaGraphDestroy(g);
         E3D_CUDA(inst);
         graph_iters = iters;
+        graph_timed = timed;
     }
 };
 

@@ -184,10 +184,12 @@ class FlowConfig:
 
 
 def run_params(max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
-               check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
+               check_every: int = 0, profile_stages: int = 0, stage_kernel: int = 0,
                min_residual_drop: float = 0.0, stall_window: int = 0, stall_below: float = 0.0) -> _lib.RunParams:
     """``e3d_run_params``: MAX_ITER, SAMPLING, MIN_RESIDUAL, MIN_AEROCOEFF_ERROR of the reference's
-    config plus the launch options and the relative residual-drop stop."""
+    config plus the launch options and the relative residual-drop stop.  ``profile_stages``: 0 CUDA
+    graphs; 1 (or True) direct launches, every stage kernel timed; 2 CUDA graphs with every stage
+    kernel timed by events captured in the graph."""
     return _lib.RunParams(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, int(profile_stages),
                           stage_kernel, min_residual_drop, stall_window, stall_below)
 
@@ -263,7 +265,7 @@ class EulerSolver:
 
     # ---- hot path
     def run(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0, min_aerocoeff_error: float = 0.0,
-            check_every: int = 0, profile_stages: bool = False, stage_kernel: int = 0,
+            check_every: int = 0, profile_stages: int = 0, stage_kernel: int = 0,
             min_residual_drop: float = 0.0, stall_window: int = 0, stall_below: float = 0.0) -> Dict[str, object]:
         rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, check_every, profile_stages,
                         stage_kernel, min_residual_drop, stall_window, stall_below)

@@ -206,8 +206,11 @@ typedef struct e3d_run_params {
 	double min_aerocoeff_error;       /* MIN_AEROCOEFF_ERROR= (0 disables the coefficient exit) */
 	int32_t check_every;              /* iterations per CUDA-graph launch between host checks of the
 	                                     stop flag (0: 32); iterations past a stop are no-ops */
-	int32_t profile_stages;           /* 1: launch directly and time every stage kernel with CUDA
-	                                     events (stats.stage_ms); 0: CUDA graphs */
+	int32_t profile_stages;           /* 0: CUDA graphs; 1: launch directly and time every stage
+	                                     kernel with CUDA events (stats.stage_ms); 2: CUDA graphs as
+	                                     with 0, with an event pair captured around every stage kernel,
+	                                     so the stages are timed as they run back to back
+	                                     (stats.stage_ms over the iterations that ran) */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
 	                                     register budgets; 3: face tiles; 4: persistent double-buffered
 	                                     face tiles; 5: face tiles at seven blocks per SM (FP64 only)

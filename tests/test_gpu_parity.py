@@ -229,6 +229,25 @@ def test_fast_kernels_agree(scheme):
             assert np.array_equal(other[0][k], states[0][0][k]), k
 
 
+def test_timed_graph():
+    """profile_stages = 2 times every stage kernel inside the graph: only the iterations that ran
+    count (12 of two 8-iteration graph launches), and the run computes what the plain graph does."""
+    name = "tets"
+    flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
+    arrays = prepared(name)
+    out = []
+    for prof in (0, 2):
+        s = EulerSolver(arrays, flow)
+        st = s.run(12, check_every=8, profile_stages=prof)
+        out.append((s.get_state(), st))
+    plain, timed = out[0][1], out[1][1]
+    assert plain["stage_launches"] == 0 and timed["iterations"] == 12
+    assert timed["stage_launches"] == 5 * 12
+    assert 0.0 < timed["stage_ms"] <= timed["device_ms"]
+    for k in STATE_KEYS:
+        assert np.array_equal(out[0][0][k], out[1][0][k]), k
+
+
 def test_autotune_info():
     name = "tets"
     s = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL))
