@@ -247,13 +247,11 @@ _KUHN = [((0, 0, 0), (1, 0, 0), (1, 1, 0), (1, 1, 1)),
          ((0, 0, 0), (0, 0, 1), (0, 1, 1), (1, 1, 1))]
 
 
-def bump_box_tets(n: int = 128, length: float = 4.0, height: float = 0.1, sigma: float = 0.3,
-                  jitter: float = 0.03, seed: int = 2, nx: int = 0, ny: int = 0, nz: int = 0) -> RawMesh:
-    """``nx x ny x nz`` (default ``n``^3) hexahedra on [0,length]^3 with a Gaussian bump of
-    ``height`` and width ``sigma`` centred on the floor (y=0), each split into 6 tetrahedra.
-    Interior nodes are jittered by +-``jitter`` of the local spacing.  Tags: floor ``wall``,
-    inlet/outlet (x) and top (y) ``farfield``, z-faces ``sym``."""
-    nx, ny, nz = nx or n, ny or n, nz or n
+def _bump_box_nodes(nx: int, ny: int, nz: int, length: float, height: float, sigma: float, jitter: float,
+                    seed: int) -> np.ndarray:
+    """Nodes of the bump box: an (nx+1) x (ny+1) x (nz+1) grid on [0,length]^3 whose floor (y=0)
+    carries a Gaussian bump of ``height`` and width ``sigma``, interior nodes jittered by
+    +-``jitter`` of the local spacing.  Node id = i + (nx+1) (j + (ny+1) k)."""
     rng = np.random.default_rng(seed)
     I = np.arange(nx + 1, dtype=np.float64)
     J = np.arange(ny + 1, dtype=np.float64)
@@ -280,6 +278,17 @@ def bump_box_tets(n: int = 128, length: float = 4.0, height: float = 0.1, sigma:
         xyz[kk * plane:(kk + 1) * plane, 0] = x.ravel()
         xyz[kk * plane:(kk + 1) * plane, 1] = y.ravel()
         xyz[kk * plane:(kk + 1) * plane, 2] = z.ravel()
+    return xyz
+
+
+def bump_box_tets(n: int = 128, length: float = 4.0, height: float = 0.1, sigma: float = 0.3,
+                  jitter: float = 0.03, seed: int = 2, nx: int = 0, ny: int = 0, nz: int = 0) -> RawMesh:
+    """``nx x ny x nz`` (default ``n``^3) hexahedra on [0,length]^3 with a Gaussian bump of
+    ``height`` and width ``sigma`` centred on the floor (y=0), each split into 6 tetrahedra.
+    Interior nodes are jittered by +-``jitter`` of the local spacing.  Tags: floor ``wall``,
+    inlet/outlet (x) and top (y) ``farfield``, z-faces ``sym``."""
+    nx, ny, nz = nx or n, ny or n, nz or n
+    xyz = _bump_box_nodes(nx, ny, nz, length, height, sigma, jitter, seed)
 
     def nid(ii, jj, kk):
         return ii + (nx + 1) * (jj + (ny + 1) * kk)
@@ -324,6 +333,70 @@ def bump_box_tets(n: int = 128, length: float = 4.0, height: float = 0.1, sigma:
     ]
     return RawMesh(xyz, np.full(tets.shape[0], VTK_TETRA, np.int32), _pack(tets, 8), markers,
                    name=f"bump_box_tets_{nx}x{ny}x{nz}")
+
+
+# faces of a VTK hexahedron, outward, in the reference's element definition order
+# (src/mesh/Mesh.hpp element face tables)
+_HEX_FACES = ((0, 3, 2, 1), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7), (4, 5, 6, 7))
+
+
+def bump_box_pyramids(n: int = 4, length: float = 4.0, height: float = 0.1, sigma: float = 0.3,
+                      jitter: float = 0.03, seed: int = 2, nx: int = 0, ny: int = 0, nz: int = 0) -> RawMesh:
+    """The bump box of :func:`bump_box_tets` in mixed elements: a hexahedron where i + j + k is
+    even, elsewhere the hexahedron split into six pyramids, one on each of its faces, with their
+    apex at a node added at its centre (the mean of its eight corners).  Every face between two
+    cells of different hexahedra is a whole quadrilateral, so the mesh is conforming; the pyramids
+    of one hexahedron meet on triangles.  A pyramid's base is its hexahedron face with the node
+    order reversed, so that the pyramid's own base face (nodes 0 3 2 1) points outward like the
+    hexahedron's.  Cells are listed hexahedron slot by slot.  Tags as in bump_box_tets."""
+    nx, ny, nz = nx or n, ny or n, nz or n
+    xyz = _bump_box_nodes(nx, ny, nz, length, height, sigma, jitter, seed)
+
+    def nid(ii, jj, kk):
+        return ii + (nx + 1) * (jj + (ny + 1) * kk)
+
+    ck, cj, ci = np.meshgrid(np.arange(nz, dtype=np.int64), np.arange(ny, dtype=np.int64),
+                             np.arange(nx, dtype=np.int64), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    corners = ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1))
+    hexes = np.stack([nid(ci + a, cj + b, ck + c) for a, b, c in corners], 1).astype(np.int32)
+    split = (ci + cj + ck) % 2 == 1
+    centre = xyz[hexes[split]].mean(axis=1)
+    apex = xyz.shape[0] + np.arange(int(split.sum()), dtype=np.int32)
+    xyz = np.concatenate([xyz, centre])
+    hs = hexes[split]
+    pyr = np.empty((hs.shape[0], 6, 5), np.int32)
+    for f, (a, b, c, d) in enumerate(_HEX_FACES):
+        pyr[:, f] = np.stack([hs[:, a], hs[:, d], hs[:, c], hs[:, b], apex], 1)
+    # cells in slot order: a whole hexahedron, or the six pyramids of a split one
+    slot = np.arange(ci.size)
+    cells = np.concatenate([_pack(hexes[~split], 8), _pack(pyr.reshape(-1, 5), 8)])
+    vtk = np.concatenate([np.full(int((~split).sum()), VTK_HEXA, np.int32),
+                          np.full(pyr.shape[0] * 6, VTK_PYRAMID, np.int32)])
+    order = np.argsort(np.concatenate([8 * slot[~split], ((8 * slot[split])[:, None] + np.arange(6)).ravel()]),
+                       kind="stable")
+
+    def face_x(ii):
+        kk, jj = np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij")
+        kk, jj = kk.ravel(), jj.ravel()
+        return np.stack([nid(ii, jj, kk), nid(ii, jj + 1, kk), nid(ii, jj + 1, kk + 1), nid(ii, jj, kk + 1)], 1)
+
+    def face_y(jj):
+        kk, ii = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+        kk, ii = kk.ravel(), ii.ravel()
+        return np.stack([nid(ii, jj, kk), nid(ii + 1, jj, kk), nid(ii + 1, jj, kk + 1), nid(ii, jj, kk + 1)], 1)
+
+    def face_z(kk):
+        jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+        jj, ii = jj.ravel(), ii.ravel()
+        return np.stack([nid(ii, jj, kk), nid(ii + 1, jj, kk), nid(ii + 1, jj + 1, kk), nid(ii, jj + 1, kk)], 1)
+
+    markers = [
+        _marker("farfield", np.concatenate([face_x(0), face_x(nx), face_y(ny)])),
+        _marker("wall", face_y(0)),
+        _marker("sym", np.concatenate([face_z(0), face_z(nz)])),
+    ]
+    return RawMesh(xyz, vtk[order], cells[order], markers, name=f"bump_box_pyramids_{nx}x{ny}x{nz}")
 
 
 # --------------------------------------------------------------------------------------------

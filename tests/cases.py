@@ -33,6 +33,7 @@ CASES = {
     "channel_supersonic": Case("channel_supersonic", lambda: mg.bump_channel(16, 8, 2, seed=5), 1.5, 2.0, 0.8),
     "ogrid": Case("ogrid", lambda: mg.biconvex_ogrid(24, 12, 2), 0.8, 1.25, 1.2),
     "tets": Case("tets", lambda: mg.bump_box_tets(5), 0.6, 0.0, 1.0),
+    "pyramids": Case("pyramids", lambda: mg.bump_box_pyramids(4), 0.6, 2.0, 1.0),
     "c1": Case("c1", lambda: mg.bump_channel(), 0.5, 0.0, 1.5),
 }
 

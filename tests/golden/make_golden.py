@@ -21,7 +21,7 @@ cp_part_0.dat, summary.txt, mesh.par.sol and mesh.par.bry, with the run's settin
 ``reference_partitions.npz`` holds the bytes of the reference's partitioned test case
 (test/mesh/StructuredBlock_8_p0..3.par) and of the mesh it was cut from.
 
-Run from the repository root:  python tests/golden/make_golden.py [integrators | outputs | partitions]
+Run from the repository root:  python tests/golden/make_golden.py [integrators | outputs | partitions | case <name>...]
 """
 import os
 import shutil
@@ -40,7 +40,7 @@ import pyoracle as po  # noqa: E402
 from cases import CASES, perturbed_state  # noqa: E402
 from euler3d_b200 import meshgen as mg  # noqa: E402
 
-GOLDEN_CASES = {"channel": 40, "channel_supersonic": 30, "ogrid": 30, "tets": 30}
+GOLDEN_CASES = {"channel": 40, "channel_supersonic": 30, "ogrid": 30, "tets": 30, "pyramids": 30}
 # (TIME_INTEGRATION=, RESIDUAL_SMOOTHING=, iterations) per variant, for these cases
 INTEGRATOR_VARIANTS = {"euler": (0, 0, 30), "euler_smooth": (0, 1, 20), "rk5_smooth": (2, 1, 10)}
 INTEGRATOR_CASES = ("channel", "ogrid", "tets")
@@ -187,6 +187,10 @@ def main():
             return
         if sys.argv[1:] == ["outputs"]:
             make_outputs(work)
+            return
+        if sys.argv[1:2] == ["case"]:  # one solver-path fixture: make_golden.py case <name>
+            for name in sys.argv[2:]:
+                print(name, make_case(name, GOLDEN_CASES[name], work), "bytes")
             return
         if sys.argv[1:] == ["partitions"]:
             make_reference_partitions(os.environ.get("E3D_REFERENCE_ROOT", "/root/reference"))

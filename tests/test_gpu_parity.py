@@ -47,7 +47,7 @@ FAST_KERNELS = KERNELS + [_lib.KERNEL_TILE_B3]  # FP64 only: face tiles at seven
 ORDERINGS = [_lib.ORDER_NATIVE, _lib.ORDER_RCM, _lib.ORDER_SPATIAL]
 
 
-@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
+@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"])
 @pytest.mark.parametrize("ordering", ORDERINGS)
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_residual_bitwise(name, ordering, kernel):
@@ -70,7 +70,7 @@ def test_residual_bitwise(name, ordering, kernel):
     assert_state_equal(gpu, o.a, m.n_cells)
 
 
-@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
+@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"])
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_rk_iteration_bitwise(name, kernel):
     """One full RK5 iteration (EulerSolver::Run body) from a perturbed state."""
@@ -264,7 +264,7 @@ def test_autotune_info():
 FP32_STATE_RTOL = 2e-5     # single-precision fluxes against the double oracle after 100 iterations
 
 
-@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
+@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"])
 def test_fp32_residual(name):
     """One residual evaluation in FP32_FLUX mode against the double oracle, relative to the largest
     face flux of the cell (single-precision rounding of each flux)."""
@@ -343,7 +343,7 @@ def test_fp32_converged_fields_and_forces():
 
 
 # ------------------------------------------------------------------ AUSM
-@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
+@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"])
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_ausm_bitwise(name, kernel):
     """AUSM in exact mode equals the oracle's restatement bit for bit (residual and one RK iteration)."""

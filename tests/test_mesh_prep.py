@@ -33,7 +33,7 @@ def raw_from_fixture(z):
     return mg.RawMesh(z["raw_xyz"], z["raw_elem_vtk"], packed, markers)
 
 
-@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets"])
+@pytest.mark.parametrize("name", ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"])
 def test_prepared_arrays_equal_reference(name):
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     ours = Mesh.from_raw(raw_from_fixture(z)).arrays()

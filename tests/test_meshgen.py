@@ -37,6 +37,20 @@ def test_bump_box_tets_conforming(n):
     assert abs(a["cell_volume"].sum() - 64.0) < 64.0 * 0.02  # [0,4]^3 minus the small bump
 
 
+@pytest.mark.parametrize("n", [2, 4])
+def test_bump_box_pyramids_conforming(n):
+    raw = mg.bump_box_pyramids(n)
+    split = sum((i + j + k) % 2 for i in range(n) for j in range(n) for k in range(n))
+    assert raw.n_cells == n ** 3 - split + 6 * split
+    assert set(np.unique(raw.elem_vtk)) == {mg.VTK_HEXA, mg.VTK_PYRAMID}
+    a = Mesh.from_raw(raw).arrays()
+    # every face is matched or on a marker: the box's 6 n^2 boundary quadrilaterals
+    assert a["n_faces"] - a["n_faces_int"] == 6 * n * n
+    assert a["wall_ghost"].size + a["farfield_ghost"].size + a["sym_ghost"].size == 6 * n * n
+    assert np.all(a["cell_volume"] > 0)
+    assert abs(a["cell_volume"].sum() - 64.0) < 64.0 * 0.02
+
+
 def test_generators_are_seeded():
     a, b = mg.bump_channel(seed=3), mg.bump_channel(seed=3)
     assert np.array_equal(a.xyz, b.xyz)

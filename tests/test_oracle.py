@@ -18,7 +18,7 @@ from euler3d_b200 import meshgen as mg
 from euler3d_b200.solver import FlowConfig
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIXTURES = ["channel", "channel_supersonic", "ogrid", "tets"]
+FIXTURES = ["channel", "channel_supersonic", "ogrid", "tets", "pyramids"]
 
 
 def load(name):
