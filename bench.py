@@ -296,7 +296,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_kernel_f32<6>"] if args.precision == "fp32" else
+                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_kernel_f32<8>"] if args.precision == "fp32" else
                                 ["stage_kernel<false,4>", "stage_kernel<false,5>", "tile_kernel<false,4>",
                                  "tile_pipe_kernel<false>", "tile_kernel<false,7>"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
@@ -329,8 +329,9 @@ def run_reference(args, rank, world):
     n = min(args.n, 24)
     raw = meshgen.bump_box_tets(n)
     cells = raw.n_cells
-    # each process runs ~10 s of reference solver iterations (about 0.1 s per RK5 iteration here)
-    K, W = max(2 * args.steps, 20), min(args.warmup, 2)
+    # each process runs ~10 s of reference solver iterations (about 0.1 s per RK5 iteration here),
+    # after at least three untimed ones
+    K, W = max(2 * args.steps, 20), max(args.warmup, 3)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     procs = max(1, min(cores, 64))
     with tempfile.TemporaryDirectory(prefix="e3dref") as d:
