@@ -156,11 +156,15 @@ class ClockSampler:
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-                power.append(float(parts[3]))
+                f_sm, f_max = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
+            sm.append(f_sm)
+            smax.append(f_max)
+            try:
+                power.append(float(parts[3]))
+            except ValueError:
+                pass
             for name, val in zip(names, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
