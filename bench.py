@@ -173,6 +173,37 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class Replicas:
+    """The bookkeeping of a run on N GPUs, one process each.  Each rank solves its own whole copy of
+    the workload (replicas: the solver path has no data-path exchange), so the only collectives are
+    the barriers around the timed region and the max over ranks of its duration; the job's rate is
+    the units every rank processed over the slowest rank's time.  ``dist`` is torch.distributed
+    (or None for one process); ``device`` holds the reduction's tensor ("cuda:i" with NCCL, "cpu"
+    with gloo)."""
+
+    def __init__(self, dist, device: str):
+        self.dist, self.device = dist, device
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    @staticmethod
+    def rate(units_per_rank: float, world: int, seconds: float) -> float:
+        """Whole-job throughput: ``units_per_rank`` on each of ``world`` ranks in ``seconds`` (the
+        max over ranks)."""
+        return units_per_rank * world / seconds
+
+
 # --------------------------------------------------------------------------------------- ours
 def run_ours(args, rank, world, local_rank):
     import numpy as np
@@ -208,16 +239,8 @@ def run_ours(args, rank, world, local_rank):
     setup_s = time.time() - t0
     K, W = args.steps, args.warmup
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    replicas = Replicas(dist, f"cuda:{local_rank}")
+    barrier, max_over_ranks = replicas.barrier, replicas.max
 
     # warm-up: same graph chunk as the timed run (the graph is instantiated here, not while timing)
     solver.run(W, check_every=K, stage_kernel=args.kernel)
@@ -236,7 +259,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     assert stats["iterations"] == K, stats
-    value = 5.0 * n_cells * K * world / (ms / 1e3)
+    value = Replicas.rate(5.0 * n_cells * K, world, ms / 1e3)
 
     # ---- stage-kernel duration for the roofline: the timed region's K-iteration graph run once
     # more, right after it, with an event pair captured around every stage kernel (on the solver's
@@ -273,7 +296,7 @@ def run_ours(args, rank, world, local_rank):
         ems = max_over_ranks(e0.elapsed_time(e1))
         assert st2["iterations"] == K
         nbytes = 8 * T * 8
-        e2e = {"value": 5.0 * n_cells * K * world / (ems / 1e3), "unit": UNIT,
+        e2e = {"value": Replicas.rate(5.0 * n_cells * K, world, ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
                "ms": ems, "note": "set_state (pinned host -> device) + run(K) + get_state (device -> pinned host)"}
 
