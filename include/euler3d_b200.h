@@ -302,9 +302,9 @@ e3d_status e3d_solver_write_summary(e3d_solver *solver, const char *path, int64_
  * each member's RMS and stop test and its force coefficients one block each of two more kernels,
  * and a step's iterations are one CUDA graph.  Every member keeps its own state, CFL, scheme, stop
  * criteria and iteration counters on the device; a member that meets its stop condition stops
- * updating at once, while the others go on.  Each member computes exactly what e3d_solver_run with
- * params->stage_kernel = 3 (face tiles) computes for it alone: same states, RMS history, counters
- * and coefficients.
+ * updating at once, while the others go on.  Each member computes exactly what e3d_solver_run
+ * computes for it alone, with any stage kernel (every stage kernel of a precision gives the same
+ * bits): same states, RMS history, counters and coefficients.
  *
  * A solver belongs to the batch from e3d_batch_add until it is retired or removed; meanwhile the
  * other e3d_solver_* calls on it fail with E3D_ERR_INVALID_ARG (e3d_solver_destroy removes it).
