@@ -843,13 +843,11 @@ __device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf 
     for (int k = 0; k < 6; k++) {
         if (e[k] == kNoContrib) break;
         const int j = e[k] >> 1;
-        if (e[k] & 1) {
+        // R -/+ F*S as one fused multiply-add by -/+1: the product is exact and the sum rounds once,
+        // so these are the bits of R - F*S or R + F*S, without a branch the cells of a warp split on
+        const double sg = (e[k] & 1) ? -1.0 : 1.0;
 #pragma unroll
-            for (int q = 0; q < 5; q++) R[q] -= fs[5 * j + q];
-        } else {
-#pragma unroll
-            for (int q = 0; q < 5; q++) R[q] += fs[5 * j + q];
-        }
+        for (int q = 0; q < 5; q++) R[q] = fma(sg, fs[5 * j + q], R[q]);
     }
     return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : rsqrt_nr(a.gamma * me.p * me.rho), R, W0, cg);
 }

@@ -236,9 +236,9 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
         for (int k = 0; k < 6; k++) {
             if (e[k] == kNoContrib) break;
             const int j = e[k] >> 1;
-            const double sg = (e[k] & 1) ? -1.0 : 1.0;
+            const double sg = (e[k] & 1) ? -1.0 : 1.0;  // fma by -/+1: the bits of R -/+ F*S (see tile_update)
 #pragma unroll
-            for (int q = 0; q < 5; q++) R[q] += sg * (double)fs[6 * j + q];
+            for (int q = 0; q < 5; q++) R[q] = fma(sg, (double)fs[6 * j + q], R[q]);
         }
         // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
         const float snd = gf * me.p * me.r;
