@@ -504,15 +504,21 @@ static void check_desc(const e3d_mesh_desc *d) {
 // Faces are drawn from 64 buckets by (left mod 8, right mod 8), eight at a time with distinct left
 // and right classes where the buckets allow, the fullest bucket first.  The order changes no
 // arithmetic: each face's flux is the same and every cell still sums its faces in its own order.
-static void bank_order(const FaceRec *rec, int n, std::vector<int> &order) {
+static void bank_order(const FaceRec *rec, int n, std::vector<int> &order, std::vector<int> &sorted) {
     const int mask = (1 << kTileLocalBits) - 1;
-    std::vector<int> bucket[64];
-    for (int i = 0; i < n; i++) {
+    auto cls = [&](int i) {
         const int l = rec[i].code & mask, r = (rec[i].code >> kTileLocalBits) & mask;
-        bucket[(l & 7) * 8 + (r & 7)].push_back(i);
-    }
-    size_t head[64] = {};
-    auto count = [&](int k) { return bucket[k].size() - head[k]; };
+        return (l & 7) * 8 + (r & 7);
+    };
+    // the faces sorted by class, in their own order within a class (a counting sort into one array)
+    int start[65] = {}, head[64];
+    for (int i = 0; i < n; i++) start[cls(i) + 1]++;
+    for (int k = 0; k < 64; k++) start[k + 1] += start[k];
+    for (int k = 0; k < 64; k++) head[k] = start[k];
+    sorted.resize(n);
+    for (int i = 0; i < n; i++) sorted[head[cls(i)]++] = i;
+    for (int k = 0; k < 64; k++) head[k] = start[k];
+    auto count = [&](int k) { return start[k + 1] - head[k]; };
     order.clear();
     int left = n, rot = 0;
     while (left > 0) {
@@ -522,7 +528,7 @@ static void bank_order(const FaceRec *rec, int n, std::vector<int> &order) {
             for (int da = 0; da < 8 && chosen < 0; da++) {
                 const int a = (rot + da) & 7;
                 if (used_l >> a & 1) continue;
-                size_t best = 0;
+                int best = 0;
                 for (int b = 0; b < 8; b++)
                     if (!(used_r >> b & 1) && count(a * 8 + b) > best) {
                         best = count(a * 8 + b);
@@ -530,14 +536,14 @@ static void bank_order(const FaceRec *rec, int n, std::vector<int> &order) {
                     }
             }
             if (chosen < 0) {  // no conflict-free choice left in this group: the fullest bucket
-                size_t best = 0;
+                int best = 0;
                 for (int k = 0; k < 64; k++)
                     if (count(k) > best) {
                         best = count(k);
                         chosen = k;
                     }
             }
-            order.push_back(bucket[chosen][head[chosen]++]);
+            order.push_back(sorted[head[chosen]++]);
             used_l |= 1u << (chosen / 8);
             used_r |= 1u << (chosen % 8);
             left--;
@@ -563,7 +569,7 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
     std::vector<int> face_local(Fint, -1), face_tile(Fint, -1);
     int max_cells = 0, max_faces = 0;
     bool ok = max_contrib > 0;
-    std::vector<int> hl, bnd, inter_slot, order;
+    std::vector<int> hl, bnd, inter_slot, order, sorted;
     std::vector<FaceRec> inter;
     for (int t = 0; t < n_tiles && ok; t++) {
         const int c0 = t * T, c1 = std::min(N, c0 + T);
@@ -608,7 +614,7 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
                                         gq.z, gq.w});
                 inter_slot.push_back(slot);
             }
-        bank_order(inter.data(), (int)inter.size(), order);
+        bank_order(inter.data(), (int)inter.size(), order, sorted);
         for (int i : order) {
             face_local[inter_slot[i]] = (int)tface.size() - fbase;
             tface.push_back(inter[i]);
