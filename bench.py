@@ -52,8 +52,13 @@ def parse():
                          "(FP32_FLUX: 3 and 4 are its two face-tile register budgets)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=["all", "stage", "served"], default="all",
-                    help="stage: the RK-stage line only; served: the served-stream comparison only")
+    ap.add_argument("--mode", choices=["all", "stage", "served", "profile"], default="all",
+                    help="stage: the RK-stage line only; served: the served-stream comparison only; profile: a "
+                         "few iterations of one stage-kernel variant (--kernel, no autotuning) on the --n mesh, "
+                         "for profiler captures of a small case")
+    ap.add_argument("--iters", type=int, default=2, help="profile mode: RK5 iterations")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of the first iteration against the CPU oracle")
     ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-rate", type=float, default=20.0, help="Poisson arrivals per second (0: burst)")
     ap.add_argument("--served-cells", type=int, nargs=2, default=(5_000, 50_000))
@@ -225,6 +230,9 @@ def run_ours(args, rank, world, local_rank):
         if rank == 0:
             print(json.dumps({"metric": "served solves/s", "n_gpus": 1, "served": served_leg(args)}), flush=True)
         return
+    if args.mode == "profile":
+        profile_case(args, local_rank)
+        return
 
     t0 = time.time()
     raw = meshgen.bump_box_tets(args.n)
@@ -300,11 +308,12 @@ def run_ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
                "ms": ems, "note": "set_state (pinned host -> device) + run(K) + get_state (device -> pinned host)"}
 
-    # ---- CPU baseline: the oracle port, one RK5 iteration of the same mesh, one core
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # ---- CPU baseline: the oracle port, one RK5 iteration of the same mesh, one core; and parity of
+    # the GPU's first iteration from the freestream with that iteration (outside every timed region)
+    cpu, parity = None, None
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline and args.no_parity):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle as po
+        import pyoracle as po  # the checker and the CPU baseline only
 
         m = po.Mesh(arrays)
         fl = po.flow(0.6, 0.0, 1.4, 1.0)
@@ -312,8 +321,11 @@ def run_ours(args, rank, world, local_rank):
         t = time.time()
         po.run(m, fl, s, 1)
         dt = time.time() - t
-        cpu = {"value": 5.0 * n_cells / dt, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"1 RK5 iteration of the full {n_cells}-cell mesh ({dt:.1f} s), CPU oracle port, 1 thread"}
+        if not args.no_cpu_baseline:
+            cpu = {"value": 5.0 * n_cells / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"1 RK5 iteration of the full {n_cells}-cell mesh ({dt:.1f} s), CPU oracle port, 1 thread"}
+        if not args.no_parity:
+            parity = first_iteration_parity(solver, arrays, flow, s.a, n_cells, args.precision)
 
     launches = stats["kernel_launches"]
     line = {
@@ -334,7 +346,7 @@ def run_ours(args, rank, world, local_rank):
                      "timing": "event pairs around every stage kernel in a second run of the timed graph",
                      "frac_alone": bytes_per_cell * n_cells / (stage_ms_alone / 1e3) / 1e9 / peak,
                      "avg_launch_ms_alone": stage_ms_alone, "autotune": solver.info()},
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "parity": parity,
     }
     solver.close()
     del arrays
@@ -345,6 +357,60 @@ def run_ours(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def first_iteration_parity(solver, arrays, flow, oracle_state, n_cells, precision):
+    """One RK5 iteration of the benchmarked mesh from the freestream on the GPU against the same
+    iteration of the CPU oracle: the largest per-cell relative difference of the interior fields
+    (velocity components relative to the local flow speed), and, for the double-precision modes, a
+    bit-for-bit check of FP64_EXACT on the same mesh."""
+    import dataclasses
+
+    import numpy as np
+
+    from euler3d_b200 import _lib
+    from euler3d_b200.solver import EulerSolver
+
+    def max_rel(g, o):
+        speed = np.sqrt(o["u"][:n_cells] ** 2 + o["v"][:n_cells] ** 2 + o["w"][:n_cells] ** 2)
+        worst = 0.0
+        for k in ("rho", "u", "v", "w", "p", "E", "H"):
+            scale = speed if k in ("u", "v", "w") else np.abs(o[k][:n_cells])
+            worst = max(worst, float(np.max(np.abs(g[k][:n_cells] - o[k][:n_cells]) / scale)))
+        return worst
+
+    solver.set_freestream()
+    solver.run(1)
+    out = {"cells": n_cells, "iterations": 1, "start": "freestream", "against": "CPU oracle (C restatement)",
+           "max_rel": max_rel(solver.get_state(), oracle_state),
+           "tolerance": 2e-5 if precision == "fp32" else 1e-10}
+    out["within_tolerance"] = out["max_rel"] <= out["tolerance"]
+    if precision != "fp32":
+        ex = EulerSolver(arrays, dataclasses.replace(flow, precision=_lib.PREC_FP64_EXACT), autotune=False)
+        ex.run(1)
+        g = ex.get_state()
+        ex.close()
+        out["fp64_exact_bitwise"] = bool(all(np.array_equal(g[k][:n_cells], oracle_state[k][:n_cells])
+                                             for k in ("rho", "u", "v", "w", "p", "E", "H")))
+    return out
+
+
+def profile_case(args, device):
+    """A few RK5 iterations of one stage-kernel variant on the --n bump box (autotuning skipped when a
+    kernel is forced, so the only stage launches are the run's), for profiler captures of a small
+    case; prints the cell count and the mean stage-kernel duration (CUDA events)."""
+    from euler3d_b200 import _lib, meshgen
+    from euler3d_b200.solver import EulerSolver, FlowConfig, Mesh
+
+    prec = {"fp64": _lib.PREC_FP64, "fp64_exact": _lib.PREC_FP64_EXACT, "fp32": _lib.PREC_FP32_FLUX}[args.precision]
+    order = {"spatial": _lib.ORDER_SPATIAL, "rcm": _lib.ORDER_RCM, "native": _lib.ORDER_NATIVE}[args.ordering]
+    arrays = Mesh.from_raw(meshgen.bump_box_tets(args.n)).arrays()
+    s = EulerSolver(arrays, FlowConfig(mach=0.6, cfl=1.0, precision=prec, ordering=order, device=device),
+                    autotune=args.kernel == 0)
+    st = s.run(args.iters, profile_stages=True, stage_kernel=args.kernel)
+    print(json.dumps({"mode": "profile", "cells": int(arrays["n_cells"]), "kernel": args.kernel,
+                      "precision": args.precision, "autotune_ms": s.info()["variant_ms"],
+                      "stage_ms": st["stage_ms"] / st["stage_launches"]}), flush=True)
 
 
 # --------------------------------------------------------------------------------------- reference

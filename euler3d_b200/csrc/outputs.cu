@@ -98,14 +98,14 @@ std::string toml_vec(const double v[3]) {
 
 // The last run's coefficient samples: 7 doubles each (iteration, force, moment).
 std::vector<double> samples_of(Solver *S) {
-    const int n = std::min(S->ctl_host->n_samples, S->sample_cap);
+    const int n = S->records_valid ? std::min(S->ctl_host->n_samples, S->sample_cap) : 0;
     std::vector<double> v(7 * (size_t)std::max(n, 0));
     if (n > 0) E3D_CUDA(cudaMemcpy(v.data(), S->samples.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost));
     return v;
 }
 
 std::vector<double> history_of(Solver *S) {
-    const int n = std::min(S->ctl_host->n_rms, S->hist_cap);
+    const int n = S->records_valid ? std::min(S->ctl_host->n_rms, S->hist_cap) : 0;
     std::vector<double> v(std::max(n, 0));
     if (n > 0) E3D_CUDA(cudaMemcpy(v.data(), S->hist.p, n * sizeof(double), cudaMemcpyDeviceToHost));
     return v;
@@ -150,6 +150,9 @@ e3d_status e3d_solver_wall_cp(e3d_solver *solver, double *cp, int32_t capacity, 
 e3d_status e3d_solver_write_residuals(e3d_solver *solver, const char *path) {
     return guarded([&] {
         Solver *S = writable(solver);
+        if (!S->records_valid)
+            throw Error(E3D_ERR_INVALID_ARG, "the last run was e3d_solver_run_noalloc, which keeps no RMS history or "
+                                             "coefficient samples in the handle");
         const Control c = *S->ctl_host;
         const std::vector<double> smp = samples_of(S), hist = history_of(S);
         OutFile o(path);

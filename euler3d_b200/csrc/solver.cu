@@ -29,6 +29,13 @@ namespace e3d {
 __device__ __forceinline__ void finalize_body(const FinalizeArgs &f, double *sh) {
     Control *ctl = f.ctl;
     if (ctl->done) return;
+    if (ctl->fault) {  // a stage kernel's bounded wait gave up: its cells kept their old state, so stop
+        if (threadIdx.x == 0) {
+            ctl->done = 1;
+            ctl->stop_reason = E3D_STOP_MAX_ITER;
+        }
+        return;
+    }
     if (f.rsq) {
         // FP64_EXACT: EulerSolver::computeRMS's own order, one running sum over the cells in
         // reference order (src/solver/EulerSolver.cpp:382-389)
@@ -1116,6 +1123,7 @@ void begin_run(Solver *S, const e3d_run_params *rp, cudaStream_t s) {
     if (S->n_wall) E3D_CUDA(cudaMemsetAsync(S->wall_cp.p, 0, S->n_wall * sizeof(double), s));
     init_control(S, rp, max_iter, S->hist_cap, S->sample_cap, s);
     state_to_buffer0(S, s);
+    S->records_valid = true;
 }
 
 void stats_from_control(const Control &c, e3d_run_stats *st) {
@@ -1422,13 +1430,18 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
         if (rp->stage_kernel != 0) throw Error(E3D_ERR_INVALID_ARG, "the no-alloc run uses the handle's stage kernel");
         if (S->euler() || S->smoothing)
             throw Error(E3D_ERR_INVALID_ARG, "the no-alloc run supports RK5 without residual smoothing only");
+        if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
         double *partials = noalloc_scratch(S->device);
         double *hist = partials + kNoAllocMaxBlocks;
         // the history region starts cleared, so no entry of an earlier call can be read back
         E3D_CUDA(cudaMemsetAsync(hist, 0, (size_t)std::max(max_iter, 1) * sizeof(double), S->stream));
-        if (!(rp->min_residual_drop >= 0.0)) throw Error(E3D_ERR_INVALID_ARG, "min_residual_drop must be >= 0");
+        // a fresh AeroCoefficients, as e3d_solver_run starts one: wall Cp zero until the first sample
+        if (S->n_wall) E3D_CUDA(cudaMemsetAsync(S->wall_cp.p, 0, S->n_wall * sizeof(double), S->stream));
         init_control(S, rp, max_iter, kNoAllocMaxIter, 0, S->stream);
         state_to_buffer0(S, S->stream);
+        // the handle's RMS history and sample record still hold an earlier run's: this run keeps
+        // neither there (its RMS history goes to rms_history), so the queries of them report none
+        S->records_valid = false;
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
         const int every = rp->check_every > 0 ? rp->check_every : 32;
         int64_t launches = 0;
@@ -1472,12 +1485,28 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
     });
 }
 
+e3d_status e3d_solver_set_wait_limit(e3d_solver *solver, int32_t polls) {
+    return guarded([&] {
+        if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");
+        Solver *S = as_solver(solver);
+        if (S->batch) throw Error(E3D_ERR_INVALID_ARG, "solver is a member of a batch (retire or remove it first)");
+        const int v = polls < 0 ? kWaitLimit : std::min<int>(polls, kWaitLimit);
+        if (v != S->wait_polls && S->graph) {  // the captured launches hold the old limit
+            E3D_CUDA(cudaSetDevice(S->device));
+            E3D_CUDA(cudaStreamSynchronize(S->stream));
+            cudaGraphExecDestroy(S->graph);
+            S->graph = nullptr;
+        }
+        S->wait_polls = v;
+    });
+}
+
 e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count) {
     return guarded([&] {
         if (!solver || !count) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
         Solver *S = solo(solver);
         E3D_CUDA(cudaSetDevice(S->device));
-        int n = std::min(S->ctl_host->n_rms, S->hist_cap);
+        int n = S->records_valid ? std::min(S->ctl_host->n_rms, S->hist_cap) : 0;
         *count = n;
         if (out && capacity > 0 && n > 0)
             E3D_CUDA(cudaMemcpy(out, S->hist.p, std::min(n, capacity) * sizeof(double), cudaMemcpyDeviceToHost));

@@ -157,6 +157,10 @@ struct Solver {
     Control *ctl_host = nullptr;   // pinned mirror
     int cur = 0;                   // q buffer holding the current state
     int hist_cap = 0;
+    // the RMS history and coefficient samples on the device are the last run's (false after an
+    // e3d_solver_run_noalloc, which keeps neither in the handle)
+    bool records_valid = true;
+    int wait_polls = kWaitLimit;   // polls of the stage kernels' data waits (e3d_solver_set_wait_limit)
 
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
@@ -262,6 +266,7 @@ struct Solver {
         a.split = 0;
         a.r_dev = nullptr;
         a.rsq = rsq.p;
+        a.wait_polls = wait_polls;
         return a;
     }
 

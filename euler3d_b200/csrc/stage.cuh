@@ -114,6 +114,8 @@ struct StageArgs {
                                      // update phase reads the smoothed residual from here
     double *__restrict__ rsq;        // FP64_EXACT: R_rho^2 of every cell in reference order (last stage),
                                      // summed sequentially like EulerSolver::computeRMS; else null
+    int wait_polls;                  // polls of a tile's data barrier before the wait gives up (kWaitLimit;
+                                     // fewer, down to 0, only to exercise the timeout path)
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -850,13 +852,20 @@ __device__ __forceinline__ double tile_update(const StageArgs &a, const TileBuf 
     return finish_cell<EXACT>(a, c0 + i, me, EXACT ? 0.0 : rsqrt_nr(a.gamma * me.p * me.rho), R, W0, cg);
 }
 
-// Bounded wait on an mbarrier phase by every thread; on timeout the fault word is set.
-// Returns true for the whole block only if every thread saw the phase complete.
+// Bounded wait on an mbarrier phase by every thread (a.wait_polls polls); on timeout the fault word
+// is set.  Returns true for the whole block only if every thread saw the phase complete.
 __device__ __forceinline__ bool tile_wait(const StageArgs &a, uint64_t *bar, uint32_t parity) {
     bool ok = false;
-    for (int it = 0; it < kWaitLimit && !ok; it++) ok = mbar_try_wait(bar, parity);
+    for (int it = 0; it < a.wait_polls && !ok; it++) ok = mbar_try_wait(bar, parity);
     if (!ok) atomicExch(a.fault, 1);
     return !__syncthreads_or(!ok);
+}
+
+// After a wait gave up: let the bulk copies still in flight on bar land (bounded by kWaitLimit)
+// before the block leaves, so that nothing writes this block's shared memory after it exits.
+__device__ __forceinline__ void tile_drain(uint64_t *bar, uint32_t parity) {
+    for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, parity); it++) {
+    }
 }
 
 // ---- one block per tile, all loads issued at the start (variant 2)
@@ -897,8 +906,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *
     }
     cp_async_wait_all();
     if (!tile_wait(a, bar, 0)) {
-        for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, 0); it++) {
-        }  // let copies in flight land before the block leaves
+        tile_drain(bar, 0);
         return;
     }
     tile_fluxes<EXACT, kStageThreads>(a, b, fs, nf, c0);
@@ -1026,10 +1034,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a)
         // this tile's data: own cp.async group (all but the newest) and the bulk copies
         asm volatile("cp.async.wait_group 1;" ::: "memory");
         if (!tile_wait(a, cur ? &bars[1] : &bars[0], (uint32_t)((i >> 1) & 1))) {
+            // this tile's copies and, when it was issued, the next tile's may still be in flight
             asm volatile("cp.async.wait_all;" ::: "memory");
-            for (int it = 0; it < kWaitLimit && !mbar_try_wait(cur ? &bars[0] : &bars[1], (uint32_t)(((i + 1) >> 1) & 1));
-                 it++) {
-            }
+            tile_drain(cur ? &bars[1] : &bars[0], (uint32_t)((i >> 1) & 1));
+            if (next < n_tiles) tile_drain(cur ? &bars[0] : &bars[1], (uint32_t)(((i + 1) >> 1) & 1));
             return;
         }
         const TileBuf b = pick(cur);

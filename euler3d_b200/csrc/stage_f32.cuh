@@ -180,8 +180,7 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
     }
     cp_async_wait_all();
     if (!tile_wait(a, bar, 0)) {
-        for (int it = 0; it < kWaitLimit && !mbar_try_wait(bar, 0); it++) {
-        }
+        tile_drain(bar, 0);
         return;
     }
 

@@ -282,8 +282,9 @@ class EulerSolver:
     def run_noalloc(self, max_iter: int, sampling: int = 1, min_residual: float = 0.0,
                     min_aerocoeff_error: float = 0.0, check_every: int = 0):
         """``e3d_solver_run_noalloc``: the same iterations as :meth:`run` without any device allocation
-        (scratch in a fixed 1 MiB device array; at most 65,536 iterations per call).  Returns
-        (stats, density RMS of every iteration)."""
+        (scratch in a fixed 1.5 MiB device array; at most 65,536 iterations per call).  Returns
+        (stats, density RMS of every iteration); the handle's own RMS history and coefficient samples
+        then report no entries."""
         rp = run_params(max_iter, sampling, min_residual, min_aerocoeff_error, check_every)
         st = _lib.RunStats()
         hist = np.zeros(max(max_iter, 1))
@@ -292,6 +293,11 @@ class EulerSolver:
         stats = stats_dict(st)
         del stats["stage_ms"], stats["stage_launches"]
         return stats, hist[: st.n_rms].copy()
+
+    def set_wait_limit(self, polls: int) -> None:
+        """``e3d_solver_set_wait_limit``: polls of the stage kernels' bounded data waits (negative:
+        the default).  0 makes every wait give up at once, which exercises the timeout path."""
+        check(_lib.load().e3d_solver_set_wait_limit(self._h, polls))
 
     def rms_history(self) -> np.ndarray:
         n = C.c_int32()

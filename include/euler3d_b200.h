@@ -254,9 +254,23 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *params, e3d_
  * looks up the array's device address (cudaGetSymbolAddress), so make that first call before any
  * stream capture.  All calls share the array, so calls that overlap on the GPU race on it.  The
  * density RMS of every iteration run is copied to rms_history (up to history_capacity entries;
- * NULL skips it).  params->stage_kernel must be 0.  No counterpart in the reference. */
+ * NULL skips it).  params->stage_kernel must be 0.  After this call the state, the stats, the wall
+ * Cp (e3d_solver_wall_cp, e3d_solver_write_cp) and e3d_solver_write_summary / _write_solution are
+ * this run's; the handle keeps no RMS history or coefficient samples of it, so
+ * e3d_solver_rms_history and e3d_solver_coefficient_history report no entries and
+ * e3d_solver_write_residuals fails with E3D_ERR_INVALID_ARG until the next e3d_solver_run.
+ * No counterpart in the reference. */
 e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *params, e3d_run_stats *stats,
                                   double *rms_history, int32_t history_capacity);
+
+/* Fault-path check without a fault: the number of polls the stage kernels make on a tile's data
+ * barrier before their bounded wait gives up (default and maximum 4,194,304; a negative value
+ * restores the default).  With 0 every wait gives up at once: the kernel lets the copies it issued
+ * land, marks the run failed and returns, the run stops after that stage with E3D_ERR_TIMEOUT, and
+ * the handle stays usable.  Face-tile stage kernels only (the per-cell gather kernels never wait).
+ * Kept for later runs of this solver, also inside a batch.  No counterpart in the reference, which
+ * has no device waits. */
+e3d_status e3d_solver_set_wait_limit(e3d_solver *solver, int32_t polls);
 
 /* Density RMS of every iteration of the last e3d_solver_run (the residuals.dat column). */
 e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count);

@@ -177,6 +177,14 @@ def make_reference_meshes(work, reference_root):
     np.savez_compressed(os.path.join(HERE, "reference_test_meshes.npz"), **out)
 
 
+def reference_root() -> str:
+    """The reference's source tree, from the E3D_REFERENCE_ROOT environment variable (required)."""
+    root = os.environ.get("E3D_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("set E3D_REFERENCE_ROOT to the reference's source tree")
+    return root
+
+
 def main():
     if not po.ref_available():
         sys.exit("reference checker binary missing: run `make -C oracle ref` first")
@@ -193,13 +201,13 @@ def main():
                 print(name, make_case(name, GOLDEN_CASES[name], work), "bytes")
             return
         if sys.argv[1:] == ["partitions"]:
-            make_reference_partitions(os.environ.get("E3D_REFERENCE_ROOT", "/root/reference"))
+            make_reference_partitions(reference_root())
             return
         make_outputs(work)
         print("integrators", make_integrators(work), "bytes")
         for name, n in GOLDEN_CASES.items():
             print(name, make_case(name, n, work), "bytes")
-        ref_root = os.environ.get("E3D_REFERENCE_ROOT", "/root/reference")
+        ref_root = reference_root()
         if os.path.isdir(os.path.join(ref_root, "test", "mesh")):
             make_reference_meshes(work, ref_root)
             make_reference_partitions(ref_root)

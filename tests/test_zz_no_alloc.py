@@ -17,7 +17,7 @@ from euler3d_b200.solver import EulerSolver
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision", [_lib.PREC_FP64_EXACT, _lib.PREC_FP64])
+@pytest.mark.parametrize("precision", [_lib.PREC_FP64_EXACT, _lib.PREC_FP64, _lib.PREC_FP32_FLUX])
 @pytest.mark.parametrize("name", ["channel", "tets"])
 def test_noalloc_run_matches_run(name, precision):
     flow = CASES[name].flow(precision=precision, ordering=_lib.ORDER_SPATIAL)
@@ -36,6 +36,26 @@ def test_noalloc_run_matches_run(name, precision):
         a, b = ref.get_state(), new.get_state()
         for k in STATE_KEYS:
             assert np.array_equal(a[k], b[k]), k
+        # the wall Cp of the last sample is this call's (cleared at its start, as a run clears it)
+        assert np.array_equal(new.wall_cp(), ref.wall_cp())
+
+
+def test_noalloc_leaves_no_stale_records(tmp_path):
+    """After an allocation-free run the handle holds no RMS history or coefficient samples of it, so
+    the queries of them must not hand back an earlier e3d_solver_run's records as this run's."""
+    name = "channel"
+    s = EulerSolver(prepared(name), CASES[name].flow())
+    s.run(12, sampling=3)
+    assert s.rms_history().size == 12 and s.coefficient_history().shape[0] == 4
+    st, hist = s.run_noalloc(5, sampling=1)
+    assert hist.size == 5 and st["iterations"] == 5
+    assert s.rms_history().size == 0
+    assert s.coefficient_history().shape[0] == 0
+    with pytest.raises(_lib.E3DError) as e:
+        s.write_outputs(str(tmp_path))
+    assert e.value.status == _lib.E3D_ERR_INVALID_ARG
+    s.run(4)  # a normal run records again
+    assert s.rms_history().size == 4
 
 
 def test_noalloc_rejects_beyond_limit():
