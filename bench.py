@@ -14,9 +14,9 @@ buffers: the flow state is copied in from pinned host memory and read back every
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun, one rank per GPU): independent replicas, no data-path collective; the
-timing is the max over ranks.  ``--impl reference`` times the reference's own CPU solver
-(compiled from its sources into oracle/_ref) on a bounded sample of the same mesh family with
-one process per host core, or the CPU oracle port if that binary is absent.
+timing is the max over ranks.  ``--impl reference`` times the reference's own CPU solver program
+(compiled from its sources with its Release flags into oracle/_ref/fast) on the same mesh through
+its multi-rank MPI path, one rank per host core, or the CPU oracle port if that binary is absent.
 """
 from __future__ import annotations
 
@@ -414,61 +414,84 @@ def profile_case(args, device):
 
 
 # --------------------------------------------------------------------------------------- reference
+REF_MPI = os.path.join(ROOT, "oracle", "_ref", "fast", "e3d_ref_mpi")
+
+
+def host_cores() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def run_reference_mpi(raw, arrays, ranks: int, warm: int, iters: int, mach: float, cfl: float, workdir: str) -> dict:
+    """The reference's own solver program on ``ranks`` host cores through its multi-rank path:
+    the mesh cut into ``ranks`` x-slab partitions (.par files in the reference's layout), each rank
+    one process (shared-memory MPI), EulerSolver::Run timed by the driver over ``iters`` iterations
+    after ``warm`` untimed ones.  Built with the reference's Release flags (-Ofast)."""
+    from euler3d_b200 import meshgen
+
+    pattern = os.path.join(workdir, "part_#.par")
+    meshgen.write_partitions(raw, ranks, pattern, arrays=arrays)
+    cfg = meshgen.CaseConfig(mach=mach, aoa=0.0, cfl=cfl, max_iter=iters, sampling=1_000_000_000)
+    cfg_path = os.path.join(workdir, "case.e3d")
+    meshgen.write_e3d(cfg, cfg_path, pattern, os.path.join(workdir, "out.dat"), n_partitions=ranks)
+    env = dict(os.environ, E3D_MPI_RANKS=str(ranks))
+    r = subprocess.run([REF_MPI, cfg_path, str(warm), str(iters), "fast"], capture_output=True, text=True, env=env,
+                       cwd=workdir, start_new_session=True, timeout=3600)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("E3D_REF_MPI ")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError(f"reference run failed (rc {r.returncode}): {r.stderr[-400:]}")
+    return json.loads(lines[-1][len("E3D_REF_MPI "):])
+
+
 def run_reference(args, rank, world):
+    """``--impl reference``: the reference's own CPU solver on the bench's workload, on this host's
+    cores.  Under torchrun only rank 0 runs it."""
     if rank != 0:
         return
     from euler3d_b200 import meshgen
+    from euler3d_b200.solver import Mesh
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-
-    n = min(args.n, 24)
-    raw = meshgen.bump_box_tets(n)
+    K, W = args.steps, max(args.warmup, 3)
+    cores = host_cores()
+    raw = meshgen.bump_box_tets(args.n)
     cells = raw.n_cells
-    # each process runs ~10 s of reference solver iterations (about 0.1 s per RK5 iteration here),
-    # after at least three untimed ones
-    K, W = max(2 * args.steps, 20), max(args.warmup, 3)
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    procs = max(1, min(cores, 64))
-    with tempfile.TemporaryDirectory(prefix="e3dref") as d:
-        cfg = meshgen.CaseConfig(mach=0.6, aoa=0.0, cfl=1.0, max_iter=K, sampling=1)
-        cfg_path = meshgen.write_case(raw, cfg, d)
-        if po.ref_available():
-            kind = "reference"
-            cmd = [po.REF_DRIVER, "bench", cfg_path, str(W), str(K)]
-            t0 = time.time()
-            ps = [subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, cwd=d)
-                  for _ in range(procs)]
-            outs = [p.communicate()[0] for p in ps]
-            secs = []
-            for o in outs:
-                # the reference's last message has no newline: take the JSON object wherever it starts
-                secs.append(json.loads(o[o.rindex('{"cells"'):].splitlines()[0])["seconds"])
-            wall = time.time() - t0
-            tmax = max(secs)
-            value = 5.0 * cells * K * procs / tmax
-            sample = (f"{procs} concurrent single-rank reference solver processes (EulerSolver::Run, "
-                      f"compiled from the reference sources), each {K} RK5 iterations of a {n}^3x6 = {cells}-cell "
-                      f"mesh of the same family; slowest process {tmax:.2f} s (wall incl. setup {wall:.0f} s)")
-        else:
-            kind = "port"
-            from euler3d_b200.solver import Mesh
+    if os.path.exists(REF_MPI):
+        ranks = max(1, min(cores, 64))
+        arrays = Mesh.from_raw(raw).arrays()
+        with tempfile.TemporaryDirectory(prefix="e3dref") as d:
+            res = run_reference_mpi(raw, arrays, ranks, W, K, 0.6, 1.0, d)
+        assert res["cells"] == cells and res["iterations"] == K, res
+        tmax = res["seconds"]
+        value = 5.0 * cells * K / tmax
+        kind = "reference"
+        sample = (f"the reference's solver program (EulerSolver::Run, compiled from the reference sources with its "
+                  f"Release flags -Ofast) on the full {cells}-cell mesh, {ranks} MPI ranks (one process per host core, "
+                  f"x-slab partitions, the reference's halo exchange over a shared-memory MPI), {K} timed RK5 "
+                  f"iterations after {W} untimed; slowest rank {tmax:.2f} s; mesh connectivity set up by the "
+                  f"library's numbering-identical preparation ({res['setup_seconds']:.1f} s setup)")
+        config = {"workload": WORKLOAD, "cells": cells, "ranks": ranks, "build": "-Ofast (reference Release)",
+                  "same_mesh": True}
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po  # the CPU baseline only
 
-            arrays = Mesh.from_raw(raw).arrays()
-            m = po.Mesh(arrays)
-            fl = po.flow(0.6, 0.0, 1.4, 1.0)
-            s = po.freestream(m, fl)
-            t = time.time()
-            po.run(m, fl, s, K)
-            tmax = time.time() - t
-            procs = 1
-            value = 5.0 * cells * K / tmax
-            sample = f"CPU oracle port, {K} RK5 iterations of a {cells}-cell mesh, 1 thread"
+        arrays = Mesh.from_raw(raw).arrays()
+        m = po.Mesh(arrays)
+        fl = po.flow(0.6, 0.0, 1.4, 1.0)
+        s = po.freestream(m, fl)
+        po.run(m, fl, s, 1)
+        t = time.time()
+        po.run(m, fl, s, 1)
+        tmax = (time.time() - t) * K
+        ranks = 1
+        value = 5.0 * cells / (tmax / K)
+        kind = "port"
+        sample = (f"CPU oracle port (the reference binary is not built), 1 RK5 iteration of the full {cells}-cell "
+                  f"mesh, 1 thread, scaled to {K} steps")
+        config = {"workload": WORKLOAD, "cells": cells, "ranks": 1, "same_mesh": True}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": tmax * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample_cells": cells, "processes": procs},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+            "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ranks, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -432,91 +432,157 @@ def write_su2(mesh: RawMesh, path: str, partition: bool = True) -> None:
             f.write("NINTERNAL_MARKER= 0\n")
 
 
-def write_partitions(mesh: RawMesh, n_parts: int, pattern: str) -> List[str]:
+def _face_keys(nodes: np.ndarray) -> np.ndarray:
+    """One sortable key per face from its (k, 4) node rows (-1 padded): the sorted node ids."""
+    k = np.sort(np.where(nodes < 0, np.iinfo(np.int64).max, nodes.astype(np.int64)), axis=1)
+    return np.ascontiguousarray(k).view([("a", np.int64), ("b", np.int64), ("c", np.int64), ("d", np.int64)]).ravel()
+
+
+def _format_rows(fmt_of_count, counts: np.ndarray, values: np.ndarray) -> str:
+    """Rows of integers formatted in one pass: row i has counts[i] values and the format
+    fmt_of_count[counts[i]]; ``values`` holds the rows' values back to back."""
+    return "".join(fmt_of_count[c] for c in counts.tolist()) % tuple(values.tolist())
+
+
+def write_partitions(mesh: RawMesh, n_parts: int, pattern: str, arrays=None) -> List[str]:
     """Split ``mesh`` into ``n_parts`` slabs along x (cells by the x of their mean node) and write
     one ``.par`` file per part in the layout of the reference's partitioner (E3D_PRE,
     src/partition/Partition.cpp:150-296, src/partition/SU2Writer.cpp): each part's elements in
     ascending global order, its nodes renumbered by first use, its boundary elements, and
     NINTERNAL_MARKER sections listing every face shared with another part -- the element on each
     side (local ids) and the face's nodes in the writing part's numbering, in the same order in both
-    parts' files.  ``pattern`` contains ``#``, replaced by the part index (the reference's
-    PARTITION_FILES convention).  Coordinates are written exactly.  Returns the file paths."""
+    parts' files (the order of a loop over parts, their elements and the elements' faces).
+    ``pattern`` contains ``#``, replaced by the part index (the reference's PARTITION_FILES
+    convention).  Coordinates are written exactly.  ``arrays``: the mesh's prepared arrays, if the
+    caller has them.  Vectorised, so that meshes of 10^7 cells are written in about a minute.
+    Returns the file paths."""
     from .solver import Mesh  # the global connectivity, in the reference's numbering
 
-    a = Mesh.from_raw(mesh).arrays()
+    a = arrays if arrays is not None else Mesh.from_raw(mesh).arrays()
     n_cells = int(a["n_cells"])
-    f2c = a["face2cell"].reshape(-1, 2)
-    c2f_ptr, c2f = a["cell2face_ptr"], a["cell2face"]
-    f2n_ptr, f2n = a["face2node_ptr"], a["face2node"]
-    eptr, enodes = mesh.csr()
-    cx = np.array([mesh.xyz[enodes[eptr[e]:eptr[e + 1]], 0].mean() for e in range(n_cells)])
+    n_faces, n_int = int(a["n_faces"]), int(a["n_faces_int"])
+    f2c = np.asarray(a["face2cell"]).reshape(-1, 2).astype(np.int64)
+    c2f_ptr, c2f = np.asarray(a["cell2face_ptr"], np.int64), np.asarray(a["cell2face"], np.int64)
+    f2n_ptr, f2n = np.asarray(a["face2node_ptr"], np.int64), np.asarray(a["face2node"], np.int64)
+    npe = np.zeros(16, np.int64)
+    for v, k in NODES_PER_VTK.items():
+        npe[v] = k
+    ecount = npe[mesh.elem_vtk]
+    # x of each cell's mean node, as numpy's mean of the node x values computes it
+    cx = np.empty(n_cells)
+    xs = np.where(mesh.elem_nodes >= 0, mesh.xyz[np.maximum(mesh.elem_nodes, 0), 0], 0.0)
+    for k in np.unique(ecount).tolist():
+        sel = np.flatnonzero(ecount == k)
+        cx[sel] = xs[sel, :k].mean(axis=1)
     part = np.empty(n_cells, np.int64)
-    part[np.argsort(cx, kind="stable")] = np.arange(n_cells) * n_parts // n_cells
-    elems = [np.flatnonzero(part == p) for p in range(n_parts)]
+    part[np.argsort(cx, kind="stable")] = np.arange(n_cells, dtype=np.int64) * n_parts // n_cells
     g2l = np.empty(n_cells, np.int64)
+    elems = []
     for p in range(n_parts):
-        g2l[elems[p]] = np.arange(elems[p].size)
+        e = np.flatnonzero(part == p)
+        g2l[e] = np.arange(e.size)
+        elems.append(e)
     # local node numbering by first use over each part's elements
-    node_maps = []
+    local = []   # global -> local node id of each part (-1: not in the part)
+    inv = []     # local -> global
     for p in range(n_parts):
-        m = {}
-        for e in elems[p]:
-            for nd in enodes[eptr[e]:eptr[e + 1]]:
-                if int(nd) not in m:
-                    m[int(nd)] = len(m)
-        node_maps.append(m)
-    # boundary elements go with their interior element: match marker faces to boundary faces by node set
-    bface = {}
-    for f in range(int(a["n_faces_int"]), int(a["n_faces"])):
-        bface[frozenset(f2n[f2n_ptr[f]:f2n_ptr[f + 1]].tolist())] = int(f2c[f][0])
-    # inter-part faces in the order of the reference's loop (parts, local elements, element faces)
-    itf = [[[] for _ in range(n_parts)] for _ in range(n_parts)]
-    for p in range(n_parts):
-        for e in elems[p]:
-            for k in range(c2f_ptr[e], c2f_ptr[e + 1]):
-                f = c2f[k]
-                o = f2c[f][1] if f2c[f][0] == e else f2c[f][0]
-                if o >= n_cells or part[o] <= p:
-                    continue
-                q = int(part[o])
-                nodes = f2n[f2n_ptr[f]:f2n_ptr[f + 1]]
-                vtk = {3: 5, 4: 9}.get(len(nodes), 7)
-                itf[p][q].append([int(g2l[e]), int(g2l[o]), vtk] + [node_maps[p][int(x)] for x in nodes])
-                itf[q][p].append([int(g2l[o]), int(g2l[e]), vtk] + [node_maps[q][int(x)] for x in nodes])
+        rows = mesh.elem_nodes[elems[p]]
+        seq = rows[rows >= 0]
+        uniq, first = np.unique(seq, return_index=True)
+        g = uniq[np.argsort(first, kind="stable")]
+        m = np.full(mesh.xyz.shape[0], -1, np.int64)
+        m[g] = np.arange(g.size)
+        local.append(m)
+        inv.append(g)
+    # marker faces matched to boundary faces by node set: the part of the face's interior cell
+    bnodes = np.full((n_faces - n_int, 4), -1, np.int64)
+    bcount = f2n_ptr[n_int + 1:] - f2n_ptr[n_int:-1]
+    for k in (3, 4):
+        sel = np.flatnonzero(bcount == k)
+        bnodes[sel, :k] = f2n[f2n_ptr[n_int + sel][:, None] + np.arange(k)[None, :]]
+    bkey = _face_keys(bnodes)
+    border = np.argsort(bkey, kind="stable")
+    bsorted = bkey[border]
+    mk_part = []
+    for mk in mesh.markers:
+        nodes = np.where(np.arange(4)[None, :] < npe[mk.vtk][:, None], mk.nodes, -1)
+        key = _face_keys(nodes)
+        pos = np.minimum(np.searchsorted(bsorted, key), bsorted.size - 1)
+        if not np.all(bsorted[pos] == key):
+            raise ValueError(f"marker {mk.tag!r} has a face that is not a boundary face")
+        mk_part.append(part[f2c[n_int + border[pos], 0]])
+    # inter-part faces: every (cell, face) entry whose neighbour is an interior cell of a
+    # higher-numbered part, in the order of the loop over parts, elements and element faces
+    cell_of = np.repeat(np.arange(n_cells), np.diff(c2f_ptr))
+    fe = c2f
+    other = np.where(f2c[fe, 0] == cell_of, f2c[fe, 1], f2c[fe, 0])
+    inner = other < n_cells
+    cross = np.flatnonzero(inner & (part[cell_of] < part[np.minimum(other, n_cells - 1)]))
+    ce, co, cf = cell_of[cross], other[cross], fe[cross]
+    pp, qq = part[ce], part[co]
+    order = np.lexsort((cross, qq, pp))  # by (p, q), then loop order
+    ce, co, cf, pp, qq = ce[order], co[order], cf[order], pp[order], qq[order]
+    fcount = f2n_ptr[cf + 1] - f2n_ptr[cf]
+    fnodes = np.full((cf.size, 4), -1, np.int64)
+    for k in (3, 4):
+        sel = np.flatnonzero(fcount == k)
+        fnodes[sel, :k] = f2n[f2n_ptr[cf[sel]][:, None] + np.arange(k)[None, :]]
+    fvtk = np.where(fcount == 3, 5, np.where(fcount == 4, 9, 7))
+
+    efmt = {k: "%3d" + "%10d" * k + "%10d\n" for k in range(1, 9)}
+    ifmt = {k: "%10d" * (3 + k) + "\n" for k in range(1, 5)}
+    mfmt = {k: "%3d" + "%10d" * k + "\n" for k in range(1, 5)}
     paths = []
     for p in range(n_parts):
         path = pattern.replace("#", str(p))
-        nm = node_maps[p]
-        inv = np.empty(len(nm), np.int64)
-        for g, l in nm.items():
-            inv[l] = g
-        lines = ["%", "% Problem dimension", "%", "NDIME= 3", "%", "% Inner element connectivity", "%",
-                 f"NELEM= {elems[p].size}"]
-        for i, e in enumerate(elems[p]):
-            lines.append(f"{int(mesh.elem_vtk[e]):3d}" + "".join(f"{nm[int(x)]:10d}" for x in enodes[eptr[e]:eptr[e + 1]])
-                         + f"{i:10d}")
-        lines += ["%", "% Node coordinates", "%", f"NPOIN= {len(nm)}"]
-        for i, g in enumerate(inv):
-            lines.append("".join(f"{float(mesh.xyz[g, k])!r:>26}" for k in range(3)) + f"{i:10d}")
-        mk_lines, n_mk = [], 0
-        for mk in mesh.markers:
-            rows = []
-            for j in range(mk.vtk.size):
-                fn = mk.nodes[j][: NODES_PER_VTK[int(mk.vtk[j])]]
-                if part[bface[frozenset(fn.tolist())]] != p:
-                    continue
-                rows.append(f"{int(mk.vtk[j]):3d}" + "".join(f"{nm[int(x)]:10d}" for x in fn))
-            if rows:
-                n_mk += 1
-                mk_lines += [f"MARKER_TAG= {mk.tag}", f"MARKER_ELEMS= {len(rows)}"] + rows
-        lines += ["%", "% Boundary elements", "%", f"NMARK= {n_mk}"] + mk_lines
-        adj = [q for q in range(n_parts) if itf[p][q]]
-        lines += ["%", "% Internal Boundary elements", "%", f"NINTERNAL_MARKER= {len(adj)}"]
-        for q in adj:
-            lines += [f"INTERNAL_MARKER= {q}", f"NELEM_MPI= {len(itf[p][q])}"]
-            lines += ["".join(f"{v:10d}" for v in row) for row in itf[p][q]]
+        m = local[p]
         with open(path, "w") as f:
-            f.write("\n".join(lines) + "\n")
+            f.write("%\n% Problem dimension\n%\nNDIME= 3\n%\n% Inner element connectivity\n%\n")
+            e = elems[p]
+            f.write(f"NELEM= {e.size}\n")
+            k_e = ecount[e]
+            rows = mesh.elem_nodes[e]
+            vals = np.concatenate([mesh.elem_vtk[e][:, None].astype(np.int64), np.where(rows >= 0, m[np.maximum(rows, 0)], -1),
+                                   np.arange(e.size)[:, None]], axis=1)
+            keep = np.concatenate([np.ones((e.size, 1), bool), rows >= 0, np.ones((e.size, 1), bool)], axis=1)
+            f.write(_format_rows(efmt, k_e, vals[keep]))
+            f.write(f"%\n% Node coordinates\n%\nNPOIN= {inv[p].size}\n")
+            xyz = mesh.xyz[inv[p]]
+            vals = [x for row in zip(xyz[:, 0].tolist(), xyz[:, 1].tolist(), xyz[:, 2].tolist(), range(inv[p].size))
+                    for x in row]
+            f.write(("%26r%26r%26r%10d\n" * inv[p].size) % tuple(vals))
+            mk_text, n_mk = [], 0
+            for mk, mp in zip(mesh.markers, mk_part):
+                sel = np.flatnonzero(mp == p)
+                if sel.size == 0:
+                    continue
+                n_mk += 1
+                kk = npe[mk.vtk[sel]]
+                nodes = mk.nodes[sel]
+                keep = np.arange(4)[None, :] < kk[:, None]
+                vals = np.concatenate([mk.vtk[sel][:, None].astype(np.int64), np.where(keep, m[np.maximum(nodes, 0)], -1)],
+                                      axis=1)[np.concatenate([np.ones((sel.size, 1), bool), keep], axis=1)]
+                mk_text.append(f"MARKER_TAG= {mk.tag}\nMARKER_ELEMS= {sel.size}\n" + _format_rows(mfmt, kk, vals))
+            f.write(f"%\n% Boundary elements\n%\nNMARK= {n_mk}\n")
+            f.write("".join(mk_text))
+            # this part's side of each inter-part face: rows where it is p (cells ce) or q (cells co)
+            adj = sorted(set(qq[pp == p].tolist()) | set(pp[qq == p].tolist()))
+            f.write(f"%\n% Internal Boundary elements\n%\nNINTERNAL_MARKER= {len(adj)}\n")
+            for q in adj:
+                if p < q:
+                    sel = np.flatnonzero((pp == p) & (qq == q))
+                    mine, theirs = ce[sel], co[sel]
+                else:
+                    sel = np.flatnonzero((pp == q) & (qq == p))
+                    mine, theirs = co[sel], ce[sel]
+                kk = fcount[sel]
+                nodes = fnodes[sel]
+                keep = nodes >= 0
+                vals = np.concatenate([g2l[mine][:, None], g2l[theirs][:, None], fvtk[sel][:, None],
+                                       np.where(keep, m[np.maximum(nodes, 0)], -1)], axis=1)
+                vals = vals[np.concatenate([np.ones((sel.size, 3), bool), keep], axis=1)]
+                f.write(f"INTERNAL_MARKER= {q}\nNELEM_MPI= {sel.size}\n")
+                f.write(_format_rows(ifmt, kk, vals))
         paths.append(path)
     return paths
 
