@@ -664,9 +664,12 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
     S->tiles_ok = ok && smem <= 200 * 1024;
     int max_halo = 0;
     for (int t = 0; t < n_tiles; t++) max_halo = std::max(max_halo, halo_ptr[t + 1] - halo_ptr[t]);
-    S->pipe_smem = tile_smem_bytes(max_cells, max_faces, max_contrib, 2);
-    S->pipe_ok = S->tiles_ok && S->pipe_smem <= 227 * 1024 && max_halo <= kPipeThreads;
-    if (!S->pipe_ok) S->pipe_smem = 0;
+    // the warp-specialised kernel's ring: as many tile buffers as fit (at most eight, at least two)
+    S->ws_buffers = 0;
+    for (int nb = 8; nb >= 2 && !S->ws_buffers; nb--)
+        if (ws_smem_bytes(max_cells, max_faces, max_contrib, nb) <= 227 * 1024) S->ws_buffers = nb;
+    S->pipe_ok = ok && S->ws_buffers >= 2;
+    S->pipe_smem = S->pipe_ok ? ws_smem_bytes(max_cells, max_faces, max_contrib, S->ws_buffers) : 0;
     if (!S->tiles_ok) return;
     cudaStream_t s = S->stream;
     // halo lists at a fixed stride per tile, padded with -1: a block reads its entries without

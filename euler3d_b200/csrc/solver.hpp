@@ -19,7 +19,7 @@ void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
 void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_f32(size_t smem_bytes);
-// gather (two register budgets), face tiles, pipelined face tiles, face tiles at 7 blocks/SM
+// gather (two register budgets), face tiles, warp-specialised persistent face tiles, face tiles at 7 blocks/SM
 constexpr int kStageVariants = 5;
 
 constexpr int kReduceThreads = 256;
@@ -131,7 +131,8 @@ struct Solver {
     int w0_stride = 0;
     int halo_stride = 0;        // entries per tile of tile_halo
     bool tiles_ok = false, pipe_ok = false;
-    size_t pipe_smem = 0;
+    size_t pipe_smem = 0;      // dynamic shared memory of the warp-specialised kernel
+    int ws_buffers = 0;        // its tile buffers
     int n_tiles = 0, n_sm = 0;
     int max_contrib = 0, smem_cells = 0, smem_faces = 0;
     size_t tile_smem = 0;
@@ -257,6 +258,7 @@ struct Solver {
         a.halo_stride = halo_stride;
         a.n_tiles = n_tiles;
         a.pipe_grid = std::min(n_tiles, n_sm);
+        a.ws_buffers = ws_buffers;
         a.q32in = q32[in_buf].p;
         a.q32out = q32[1 - in_buf].p;
         a.tile_rec32 = reinterpret_cast<const char *>(tile_rec32.p);

@@ -100,7 +100,8 @@ struct StageArgs {
     int *fault;                      // set when a bounded wait gives up (reported as a timeout)
     int halo_stride;                 // entries per tile in tile_halo (the largest halo)
     int n_tiles;                     // tiles of the mesh
-    int pipe_grid;                   // tile_pipe_kernel: persistent blocks (one per SM)
+    int pipe_grid;                   // tile_ws_kernel: persistent blocks (one per SM)
+    int ws_buffers;                  // tile_ws_kernel: tile buffers in shared memory
     // FP32_FLUX mode: float cell records (rho,u,v,w | p,H,sqrt(rho),rsqrt(gamma p rho)), float
     // face records and float cell geometry; W0 stays double
     const float4 *__restrict__ q32in;
@@ -772,9 +773,10 @@ __device__ __forceinline__ Prim tile_prim(const double2 *st, int i) {
 // before the fluxes would cost a barrier phase and 16 bytes of shared memory per local cell, and
 // measured slower on B200.
 template <bool EXACT, int NT>
-__device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, double *fs, int nf, int c0) {
+__device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b, double *fs, int nf, int c0,
+                                            int tid) {
     const double g = a.gamma;
-    for (int j = threadIdx.x; j < nf; j += NT) {
+    for (int j = tid; j < nf; j += NT) {
         const FaceRec fr = b.rec[j];
         const int l = fr.code & ((1 << kTileLocalBits) - 1);
         const int r = (fr.code >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
@@ -909,7 +911,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, int tile, double *
         tile_drain(bar, 0);
         return;
     }
-    tile_fluxes<EXACT, kStageThreads>(a, b, fs, nf, c0);
+    tile_fluxes<EXACT, kStageThreads>(a, b, fs, nf, c0, threadIdx.x);
     double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
     if ((int)threadIdx.x < nloc) tile_load_cell(a, c0, threadIdx.x, W0, cg);
@@ -967,94 +969,162 @@ __global__ void __launch_bounds__(kStageThreads, MINB) tile_batch_kernel(BatchSt
     tile_body<EXACT>(sa, e.y, sa.partials + e.y, smem_raw);
 }
 
-// ---- persistent, double-buffered (variant 3)
-// One block of kPipeThreads per SM walks tiles blockIdx.x, +gridDim.x, ...  While it evaluates
-// tile i from one buffer, the bulk copies and halo gathers of tile i+1 fill the other, so memory
-// traffic overlaps computation.  Halo indices are read into registers one tile ahead of their use.
-// Shared memory: TileBuf x 2 (face fluxes over each buffer's records) | mbarrier x 2
-constexpr int kPipeThreads = 512;
+// ---- warp-specialised, persistent (variant 3)
+// One block per SM: a producer warp and kWsGroups consumer groups of kTileCells threads, over a ring
+// of `ws_buffers` tile buffers in shared memory.  The block walks tiles blockIdx.x, + gridDim.x, ...;
+// its k-th tile fills buffer k % B and is evaluated by consumer group k % G.  The producer warp
+// streams tiles ahead of the consumers: for each tile it waits until the tile's buffer is free
+// (empty barrier), then issues every copy the tile needs onto the buffer's full barrier -- the
+// owned states, face records and contribution lists as bulk copies, each halo state as a 48-byte
+// bulk copy (no multicast), and L2 prefetches of the W0 rows and cell geometry.  A consumer group
+// waits for its tile's full barrier, evaluates the fluxes and the update as tile_body does, with a
+// named barrier of its own between the phases, and hands the buffer back.  So copies for the next
+// tiles are in flight while every group computes, with no block launch, barrier initialisation or
+// index chase between tiles.  Every wait is bounded: a consumer that gives up sets the fault word and
+// leaves; the producer stops issuing once the fault word is set or its own wait gives up, and lets
+// every copy it issued land before it leaves.
+constexpr int kWsGroups = 5;
+constexpr int kWsThreads = 32 + kWsGroups * kTileCells;
+
+__host__ __device__ __forceinline__ size_t ws_buffer_bytes(int LC, int FC, int MC) {
+    return (tile_buf_bytes(LC, FC, MC) + 127) & ~(size_t)127;
+}
+
+// Dynamic shared memory of tile_ws_kernel with B buffers: the buffers, a full and an empty mbarrier
+// per buffer, and four doubles per consumer group for its RMS partial.
+inline size_t ws_smem_bytes(int smem_cells, int smem_faces, int max_contrib, int buffers) {
+    return (size_t)buffers * ws_buffer_bytes(smem_cells, smem_faces, max_contrib) + 16 * (size_t)buffers +
+           32 * (size_t)kWsGroups;
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Named barrier of `threads` threads that also returns, to all of them, whether any passed true.
+__device__ __forceinline__ bool named_sync_or(int id, int threads, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(threads)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bulk copy of one 48-byte halo state (16-byte aligned at both ends).
+__device__ __forceinline__ void ws_halo_copy(const StageArgs &a, double2 *dst, int h, uint64_t *bar) {
+    bulk_g2s(dst, a.qin + 3 * (size_t)h, 48u, bar);
+}
 
 template <bool EXACT>
-__global__ void __launch_bounds__(kPipeThreads, 1) tile_pipe_kernel(StageArgs a) {
-    const int n_tiles = a.n_tiles;
+__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
     if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
-    const size_t bb = (tile_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
-    const TileBuf buf0 = tile_buf_at(smem_raw, LC, FC, MC), buf1 = tile_buf_at(smem_raw + bb, LC, FC, MC);
-    auto pick = [&](int k) {  // select, not index: keeps the descriptors in registers
-        TileBuf r;
-        r.st = k ? buf1.st : buf0.st;
-        r.rec = k ? buf1.rec : buf0.rec;
-        r.ct = k ? buf1.ct : buf0.ct;
-        return r;
-    };
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + 2 * bb);
-    const int G = gridDim.x;
-    int tile = blockIdx.x;
-    if (tile >= n_tiles) return;
-
+    const int B = a.ws_buffers, n_tiles = a.n_tiles, G = gridDim.x;
+    const size_t bb = ws_buffer_bytes(LC, FC, MC);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)B * bb);
+    uint64_t *empty = full + B;
+    double *gsum = reinterpret_cast<double *>(empty + B);  // [kWsGroups][4]
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int k = 0; k < B; k++) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], 1);
+        }
     }
     __syncthreads();
-    auto halo_index = [&](int t) {  // this thread's halo cell of tile t, or -1
-        if (t >= n_tiles) return -1;
-        return (int)threadIdx.x < a.halo_stride ? a.tile_halo[(size_t)t * a.halo_stride + threadIdx.x] : -1;
-    };
-    auto issue = [&](int t, const TileBuf &tb, uint64_t *bar) {
-        tile_issue_bulk(a, t, a.tile_face_ptr[t + 1] - a.tile_face_ptr[t], a.tile_rec_off[t], tb, bar);
-    };
-    // prologue: tile 0 of this block in flight, halo indices of tile 1 on their way
-    if (threadIdx.x == 0) issue(tile, buf0, &bars[0]);
-    {
-        const int h = halo_index(tile);
-        if (h >= 0) tile_gather_halo(a, buf0, min(T, a.n_cells - tile * T), threadIdx.x, h);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    int h_next = halo_index(tile + G);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    for (int i = 0; tile < n_tiles; i++, tile += G) {
-        const int cur = i & 1;
-        const int next = tile + G;
-        // fill the other buffer with the next tile (its previous contents were released at the end of
-        // the last iteration)
-        if (next < n_tiles) {
-            const TileBuf nb = pick(cur ^ 1);
-            if (threadIdx.x == 0) {
-                // the buffer was last read by ordinary loads; order those before the async-proxy writes
+    if (warp == 0) {  // ------------------------------------------------ producer
+        int issued = 0;  // tiles whose copies were issued (buffer of tile k: k % B)
+        bool stop = false;
+        for (int k = 0, tile = blockIdx.x; tile < n_tiles && !stop; k++, tile += G) {
+            const int bi = k % B;
+            if (k >= B) {  // the buffer's previous tile (k - B) has been handed back
+                // lane 0 waits and the warp follows its answer, so every decision is warp-uniform
+                int ok = 0;
+                if (lane == 0) {
+                    const uint32_t par = (uint32_t)(((k / B) - 1) & 1);
+                    for (int it = 0; it < kWaitLimit && !ok; it++) {
+                        ok = mbar_try_wait(&empty[bi], par);
+                        if (!ok && (it & 255) == 255 && *(volatile int *)a.fault) break;
+                    }
+                    if (!ok) atomicExch(a.fault, 1);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    stop = true;
+                    break;
+                }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(next, nb, cur ? &bars[0] : &bars[1]);
             }
-            if (h_next >= 0) tile_gather_halo(a, nb, min(T, a.n_cells - next * T), threadIdx.x, h_next);
+            const TileBuf b = tile_buf_at(smem_raw + (size_t)bi * bb, LC, FC, MC);
+            const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
+            const int nh = a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
+            if (lane == 0) {
+                const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+                const uint32_t bytes = (uint32_t)nloc * 48u + round16(40u * (uint32_t)nf) + (uint32_t)MC * T * 2u +
+                                       (uint32_t)nh * 48u;
+                mbar_expect_tx(&full[bi], bytes);
+                bulk_g2s(b.st, a.qin + 3 * (size_t)c0, (uint32_t)nloc * 48u, &full[bi]);
+                bulk_g2s(b.rec, a.tile_rec + a.tile_rec_off[tile], round16(40u * (uint32_t)nf), &full[bi]);
+                bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, (uint32_t)MC * T * 2u, &full[bi]);
+                const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
+                for (int q = 0; q < 5; q++) bulk_prefetch_l2(a.w0 + (size_t)q * a.w0_stride + c0, b_w0);
+                bulk_prefetch_l2(a.cgeo + c0, (uint32_t)nloc * 32u);
+            }
+            __syncwarp();  // the expected byte count is posted before any halo copy can complete
+            const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+            for (int i = lane; i < nh; i += 32) ws_halo_copy(a, b.st + 3 * (nloc + i), hrow[i], &full[bi]);
+            issued = k + 1;
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        h_next = halo_index(next + G);  // consumed one iteration from now
-        // this tile's data: own cp.async group (all but the newest) and the bulk copies
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
-        if (!tile_wait(a, cur ? &bars[1] : &bars[0], (uint32_t)((i >> 1) & 1))) {
-            // this tile's copies and, when it was issued, the next tile's may still be in flight
-            asm volatile("cp.async.wait_all;" ::: "memory");
-            tile_drain(cur ? &bars[1] : &bars[0], (uint32_t)((i >> 1) & 1));
-            if (next < n_tiles) tile_drain(cur ? &bars[0] : &bars[1], (uint32_t)(((i + 1) >> 1) & 1));
-            return;
+        // every copy issued must land before the block can leave (the consumers normally wait for
+        // them; after a fault they may not have)
+        if (lane == 0 && *(volatile int *)a.fault) {
+            for (int k = (issued > B ? issued - B : 0); k < issued; k++)
+                tile_drain(&full[k % B], (uint32_t)((k / B) & 1));
         }
-        const TileBuf b = pick(cur);
+        return;
+    }
+
+    // ------------------------------------------------------------------ consumer group
+    const int grp = warp - 1 >= 0 ? (threadIdx.x - 32) / T : 0;
+    const int tid = (threadIdx.x - 32) % T;
+    const int bar_id = 1 + grp;
+    double *fsum = gsum + 4 * grp;
+    for (int k = grp, tile = blockIdx.x + grp * G; tile < n_tiles; k += kWsGroups, tile += kWsGroups * G) {
+        const int bi = k % B;
+        bool ok = false;
+        for (int it = 0; it < a.wait_polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)((k / B) & 1));
+        if (!ok) atomicExch(a.fault, 1);
+        if (named_sync_or(bar_id, T, !ok)) return;  // the same decision for the whole group
+        const TileBuf b = tile_buf_at(smem_raw + (size_t)bi * bb, LC, FC, MC);
         const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
         const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
         double *fs = reinterpret_cast<double *>(b.rec);
-        tile_fluxes<EXACT, kPipeThreads>(a, b, fs, nf, c0);
+        tile_fluxes<EXACT, kTileCells>(a, b, fs, nf, c0, tid);
         double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
-        if ((int)threadIdx.x < nloc) tile_load_cell(a, c0, threadIdx.x, W0, cg);
-        __syncthreads();
+        if (tid < nloc) tile_load_cell(a, c0, tid, W0, cg);
+        named_sync(bar_id, T);
         double r2 = 0.0;
-        if ((int)threadIdx.x < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, threadIdx.x, W0, cg);
-        if (a.last_stage && !a.residual_only) block_sum_store<kPipeThreads>(r2, a.partials + tile);
-        __syncthreads();  // buffer cur (with its fluxes) is free again
+        if (tid < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, tid, W0, cg);
+        named_sync(bar_id, T);  // every read of the buffer is done
+        if (tid == 0) mbar_arrive(&empty[bi]);
+        if (a.last_stage && !a.residual_only) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+            if ((tid & 31) == 0) fsum[tid >> 5] = r2;
+            named_sync(bar_id, T);
+            if (tid == 0) a.partials[tile] = (fsum[0] + fsum[1]) + (fsum[2] + fsum[3]);
+            named_sync(bar_id, T);  // fsum is reused by the next tile
+        }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // ---- update phase of a split stage
@@ -1081,10 +1151,10 @@ __global__ void __launch_bounds__(kStageThreads) update_kernel(StageArgs a) {
     if (a.last_stage) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
-// Dynamic shared memory of tile_kernel (buffers = 1) and tile_pipe_kernel (buffers = 2).
-inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib, int buffers = 1) {
+// Dynamic shared memory of tile_kernel.
+inline size_t tile_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
     const size_t bb = (tile_buf_bytes(smem_cells, smem_faces, max_contrib) + 15) & ~(size_t)15;
-    return buffers * bb + 16;  // + one mbarrier per buffer
+    return bb + 16;  // + its mbarrier
 }
 
 }  // namespace e3d

@@ -8,7 +8,7 @@ namespace e3d {
 // Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes) {
     raise_smem_limit((const void *)tile_kernel<true, 4>, smem_bytes);
-    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<true>, pipe_smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<true>, pipe_smem_bytes);
 }
 
 void prepare_batch_exact(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<true, 4>, smem_bytes); }
@@ -24,12 +24,12 @@ void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaS
 }
 
 // variant 0: gather kernel, registers for 2 blocks/SM; 1: gather kernel, 4 blocks/SM;
-// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and double-buffered
+// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and warp-specialised
 void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
     if (variant == 3) {
-        const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, 2);
-        tile_pipe_kernel<true><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
+        const size_t smem = ws_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, a.ws_buffers);
+        tile_ws_kernel<true><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<true, 4><<<blocks, kStageThreads, smem, s>>>(a);

@@ -9,7 +9,7 @@ namespace e3d {
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     raise_smem_limit((const void *)tile_kernel<false, 4>, smem_bytes);
     raise_smem_limit((const void *)tile_kernel<false, 7>, smem_bytes);
-    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_pipe_kernel<false>, pipe_smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<false>, pipe_smem_bytes);
 }
 
 void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false, 6>, smem_bytes); }
@@ -25,7 +25,7 @@ void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaSt
 }
 
 // variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;
-// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and double-buffered;
+// 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and warp-specialised;
 // 4: face tiles with registers for 7 blocks/SM
 void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
@@ -33,8 +33,8 @@ void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false, 7><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 3) {
-        const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, 2);
-        tile_pipe_kernel<false><<<a.pipe_grid, kPipeThreads, smem, s>>>(a);
+        const size_t smem = ws_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, a.ws_buffers);
+        tile_ws_kernel<false><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false, 4><<<blocks, kStageThreads, smem, s>>>(a);

@@ -212,9 +212,10 @@ typedef struct e3d_run_params {
 	                                     so the stages are timed as they run back to back
 	                                     (stats.stage_ms over the iterations that ran) */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
-	                                     register budgets; 3: face tiles; 4: persistent double-buffered
-	                                     face tiles; 5: face tiles at seven blocks per SM (FP64 only)
-	                                     (kept for later runs) */
+	                                     register budgets; 3: face tiles; 4: persistent face tiles with
+	                                     a producer warp streaming tiles to consumer warps (FP64 modes;
+	                                     in FP32_FLUX: face tiles at eight blocks per SM); 5: face tiles
+	                                     at seven blocks per SM (FP64 only) (kept for later runs) */
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
 	                                     No counterpart in the reference, whose test is absolute. */
