@@ -7,6 +7,8 @@
                                       # residual drop at checkpoints, the FP32 fields and lift / drag
                                       # against FP64 after the same iterations, and where the FP32
                                       # residual stalls
+  python -m euler3d_b200.report c5    # the served stream at its stated sizes (10k-2M cells), FP64
+                                      # and ladder served against the plain path, per tolerance
   python -m euler3d_b200.report c4    # 256 uneven instances (bump channels and biconvex O-grids of
                                       # 5k-200k cells, Mach 0.3-0.85, AoA -4..6, Roe/AUSM) run as
                                       # one batch to a 1e-8 drop, FP32_FLUX then FP64, against the
@@ -118,12 +120,38 @@ def c4(n=256, max_iter=20_000, plain_sample=32):
     row["sample_diffs"] = {k: d[k] for k in ("max_rel_diff_cl", "max_rel_diff_cd", "converged_max_rel_diff_cl",
                                              "converged_max_rel_diff_cd", "same_outcome")}
     row["speedup_solves_per_s"] = b["solves_per_s"] / p["solves_per_s"]
+    # converged solves only: the rate of solves that reached the 1e-8 drop, batch against plain
+    row["speedup_converged_solves_per_s"] = (b["converged_solves_per_s"] / p["converged_solves_per_s"]
+                                             if p["converged"] else None)
     return [row]
+
+
+def c5(n=64, rate=20.0, max_iter=20_000):
+    """The served request stream at its stated size distribution: n requests (Poisson arrivals at
+    `rate` per second, seed 4), meshes of 10k-2M cells log-uniform (bump channels and biconvex
+    O-grids; O-grid requests above 1M cells get a channel, see serve.request_mesh), Mach 0.3-0.85,
+    AoA -4..6, Roe or AUSM, tolerance 1e-6 or 1e-8, admission by device-memory footprint under a
+    150 GB budget.  Served in FP64 and with the FP32 -> FP64 precision ladder, then solved one at a
+    time by the plain FP64 path; solves/s, p50/p99 latency, and converged solves/s for each
+    tolerance apart.  The stated stream runs 600 s (12,000 requests); this is its first n."""
+    reqs = serve.request_stream(n, rate, cells=(10_000, 2_000_000), seed=4, drops=(1e-6, 1e-8),
+                                schemes=(_lib.SCHEME_ROE, _lib.SCHEME_AUSM))
+    out = serve.compare(reqs, _lib.PREC_FP64, max_iter=max_iter, ladder=True, hbm_budget=150e9)
+    out["config"] = "c5"
+    out["workload"] = (f"{n} requests, Poisson {rate:g}/s (seed 4), cells log-uniform [10000, 2000000], "
+                       f"Mach 0.3-0.85, AoA -4..6, Roe/AUSM, drop 1e-6/1e-8, max_iter {max_iter}, 150 GB budget")
+    out["cells_total"] = int(sum(q.cells for q in reqs))
+    for key in ("served", "served_ladder"):
+        if key in out and "plain" in out:
+            out[key]["speedup_converged_solves_per_s"] = (
+                out[key]["converged_solves_per_s"] / out["plain"]["converged_solves_per_s"]
+                if out["plain"]["converged"] else None)
+    return [out]
 
 
 def main(argv=None):
     which = (argv or sys.argv[1:] or ["c1"])[0]
-    rows = {"c1": c1, "c2": c2, "c4": c4}[which]()
+    rows = {"c1": c1, "c2": c2, "c4": c4, "c5": c5}[which]()
     for r in rows:
         print(json.dumps(r), flush=True)
 

@@ -58,6 +58,7 @@ class SolveResult:
     last_rms: float
     device_bytes: int
     fp32_iterations: int = 0  # ladder: iterations of the FP32_FLUX phase
+    drop: float = 0.0         # the request's residual-drop tolerance
 
     @property
     def latency(self) -> float:
@@ -146,8 +147,20 @@ def summarize(results: Sequence[SolveResult], t_end: Optional[float] = None) -> 
     t1 = t_end if t_end is not None else max(r.finished for r in results)
     lat = [r.latency for r in results]
     span = max(t1 - t0, 1e-9)
-    converged = sum(r.status == _lib.E3D_OK and r.stop_reason == _lib.STOP_RESIDUAL for r in results)
-    return {"solves": len(results), "seconds": t1 - t0, "solves_per_s": len(results) / span,
+    def conv(r):
+        return r.status == _lib.E3D_OK and r.stop_reason == _lib.STOP_RESIDUAL
+
+    converged = sum(conv(r) for r in results)
+    # the solves of each tolerance apart: how many reached it, at what rate, with what latency
+    by_drop = {}
+    for d in sorted({r.drop for r in results}):
+        rs = [r for r in results if r.drop == d]
+        ok = [r for r in rs if conv(r)]
+        by_drop[f"{d:g}"] = {"requests": len(rs), "converged": len(ok), "converged_solves_per_s": len(ok) / span,
+                             "p50_latency_s": percentile([r.latency for r in rs], 50),
+                             "p99_latency_s": percentile([r.latency for r in rs], 99),
+                             "converged_p50_latency_s": percentile([r.latency for r in ok], 50)}
+    return {"solves": len(results), "seconds": t1 - t0, "solves_per_s": len(results) / span, "by_drop": by_drop,
             "converged": converged, "converged_solves_per_s": converged / span,
             "capped": sum(r.status == _lib.E3D_OK and r.stop_reason == _lib.STOP_MAX_ITER for r in results),
             "diverged": sum(r.status == _lib.E3D_ERR_NONFINITE for r in results),
@@ -212,7 +225,8 @@ class Server:
             req = m["req"]
             cl, cd, cm = final_coefficients(s)
             r = SolveResult(req.rid, s.n_cells, req.arrival, m["admitted"], self.clock() - t0, iterations,
-                            st["stop_reason"], status, cl, cd, cm, st["last_rms"], m["bytes"], fp32_iterations)
+                            st["stop_reason"], status, cl, cd, cm, st["last_rms"], m["bytes"], fp32_iterations,
+                            drop=req.drop)
             results.append(r)
             if on_result:
                 on_result(r, s)
@@ -237,7 +251,7 @@ class Server:
                         ready.popleft()
                         results.append(SolveResult(req.rid, int(arrays["n_cells"]), req.arrival, math.nan,
                                                    self.clock() - t0, 0, -1, _lib.E3D_ERR_OOM, math.nan, math.nan,
-                                                   math.nan, math.nan, est))
+                                                   math.nan, math.nan, est, drop=req.drop))
                         continue
                     if used + est > self.budget:
                         break
@@ -346,7 +360,8 @@ def serve_plain(requests: Sequence[SolveRequest], device: int = 0, precision: in
             finished = clock() - t0
             cl, cd, cm = final_coefficients(s)
             r = SolveResult(req.rid, s.n_cells, req.arrival, started, finished, st["iterations"],
-                            st["stop_reason"], status, cl, cd, cm, st["last_rms"], int(s.info()["device_bytes"]))
+                            st["stop_reason"], status, cl, cd, cm, st["last_rms"], int(s.info()["device_bytes"]),
+                            drop=req.drop)
             results.append(r)
             if on_result:
                 on_result(r, s)
