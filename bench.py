@@ -52,10 +52,14 @@ def parse():
                          "(FP32_FLUX: 3 and 4 are its two face-tile register budgets)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=["all", "stage", "served", "profile"], default="all",
+    ap.add_argument("--mode", choices=["all", "stage", "served", "profile", "kernels"], default="all",
                     help="stage: the RK-stage line only; served: the served-stream comparison only; profile: a "
                          "few iterations of one stage-kernel variant (--kernel, no autotuning) on the --n mesh, "
-                         "for profiler captures of a small case")
+                         "for profiler captures of a small case; kernels: a few launches of every other kernel "
+                         "(residual smoothing, state transfers, batch stage / RMS / coefficients / control) on "
+                         "small cases, for profiler captures")
+    ap.add_argument("--batch-kernel", choices=["tiles", "ws"], default="tiles",
+                    help="kernels mode: the batch stage kernel (one block per tile, or warp-specialised)")
     ap.add_argument("--iters", type=int, default=2, help="profile mode: RK5 iterations")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the first iteration against the CPU oracle")
@@ -232,6 +236,9 @@ def run_ours(args, rank, world, local_rank):
         return
     if args.mode == "profile":
         profile_case(args, local_rank)
+        return
+    if args.mode == "kernels":
+        kernels_case(args, local_rank)
         return
 
     t0 = time.time()
@@ -411,6 +418,51 @@ def profile_case(args, device):
     print(json.dumps({"mode": "profile", "cells": int(arrays["n_cells"]), "kernel": args.kernel,
                       "precision": args.precision, "autotune_ms": s.info()["variant_ms"],
                       "stage_ms": st["stage_ms"] / st["stage_launches"]}), flush=True)
+
+
+def kernels_case(args, device):
+    """A few launches of each kernel that is not a solo stage kernel, on small cases, for profiler
+    captures: explicit Euler with residual smoothing on the --n bump box (residual phase, two
+    smoothing passes, update), the state loaders and readers (FP64 and FP32_FLUX), and a batch of 64
+    bump channels of 19,600 cells in FP64 and in FP32_FLUX (batch stage, RMS, coefficient and
+    control-gather kernels; --batch-kernel chooses the FP64 stage kernel).  Prints the device time of
+    each part, and the batch stage throughput."""
+    from euler3d_b200 import _lib, meshgen
+    from euler3d_b200.batch import Batch
+    from euler3d_b200.solver import EulerSolver, FlowConfig, Mesh
+
+    out = {"mode": "kernels"}
+    arrays = Mesh.from_raw(meshgen.bump_box_tets(args.n)).arrays()
+    out["cells"] = int(arrays["n_cells"])
+    sm = EulerSolver(arrays, FlowConfig(mach=0.6, cfl=1.0, precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL,
+                                        integrator=_lib.INTEGRATOR_EULER, smoothing=True, device=device),
+                     autotune=False)
+    out["smoothing_ms"] = sm.run(args.iters)["device_ms"]
+    sm.set_state(sm.get_state())
+    sm.close()
+    f32 = EulerSolver(arrays, FlowConfig(mach=0.6, cfl=1.0, precision=_lib.PREC_FP32_FLUX,
+                                         ordering=_lib.ORDER_SPATIAL, device=device), autotune=False)
+    f32.set_state(f32.get_state())
+    f32.close()
+    ch = Mesh.from_raw(meshgen.bump_channel(140, 70, 2)).arrays()
+    for prec, name in ((_lib.PREC_FP64, "fp64"), (_lib.PREC_FP32_FLUX, "fp32")):
+        b = Batch(device)
+        if prec == _lib.PREC_FP64 and args.batch_kernel == "ws":
+            b.set_kernel(_lib.BATCH_KERNEL_WS)
+        members = [EulerSolver(ch, FlowConfig(mach=0.3 + 0.005 * i, cfl=1.5, precision=prec, ordering=_lib.ORDER_SPATIAL,
+                                              device=device), autotune=False) for i in range(64)]
+        for m in members:
+            b.add(m, 4 * args.iters)
+        b.step(args.iters)
+        b.step(args.iters)
+        ms = b.info()["last_step_ms"]
+        it = args.iters + (args.iters & 1)
+        out[f"batch_{name}_step_ms"] = ms
+        out[f"batch_{name}_cell_stages_per_s"] = 5.0 * it * 64 * int(ch["n_cells"]) / (ms / 1e3)
+        b.close()
+        for m in members:
+            m.close()
+    print(json.dumps(out), flush=True)
 
 
 # --------------------------------------------------------------------------------------- reference

@@ -19,6 +19,7 @@ ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE, KERNEL_TILE_B3 = 0, 1, 2, 3, 4, 5
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS, STOP_STALL = 0, 1, 2, 3
 INTEGRATOR_RK5, INTEGRATOR_EULER = 0, 1
+BATCH_KERNEL_TILES, BATCH_KERNEL_WS = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -114,6 +115,7 @@ SIGNATURES = {
     "e3d_mesh_read_partitions": (C.c_int, [C.POINTER(C.c_char_p), C.c_int32, C.c_double, C.c_int32,
                                            C.POINTER(C.c_void_p)]),
     "e3d_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "e3d_batch_set_kernel": (C.c_int, [C.c_void_p, C.c_int32]),
     "e3d_batch_destroy": (None, [C.c_void_p]),
     "e3d_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RunParams)]),
     "e3d_batch_step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),

@@ -35,6 +35,11 @@ class Batch:
         except Exception:
             pass
 
+    def set_kernel(self, kernel: int) -> None:
+        """``e3d_batch_set_kernel``: BATCH_KERNEL_TILES (one block per member tile) or BATCH_KERNEL_WS
+        (the warp-specialised persistent kernel; FP64 modes)."""
+        check(_lib.load().e3d_batch_set_kernel(self._h, kernel))
+
     def __len__(self) -> int:
         return len(self._members)
 

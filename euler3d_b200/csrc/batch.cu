@@ -54,6 +54,12 @@ struct Batch {
     int *one_host = nullptr;      // pinned constant 1 (sets a member's done flag)
     int member_cap = 0, tile_cap = 0;
     size_t smem_cap = 0;
+    // stage kernel: E3D_BATCH_KERNEL_TILES (one block per table entry) or E3D_BATCH_KERNEL_WS (the
+    // warp-specialised persistent kernel walking the table, FP64 modes); its ring of buffers
+    int kernel = E3D_BATCH_KERNEL_TILES;
+    int n_sm = 0;
+    int ws_buffers = 0;
+    size_t ws_stride = 0, ws_smem = 0;
     int n_entries = 0;
     bool dirty = true;
 
@@ -146,6 +152,18 @@ struct Batch {
             drop_graph();
             smem_cap = smem;
         }
+        // the warp-specialised kernel's buffers: the largest member's tile data plus its arguments
+        size_t stride = 0;
+        for (const Member &m : members)
+            stride = std::max(stride, kWsArgsSlot + ws_buffer_bytes(m.S->smem_cells, m.S->smem_faces, m.S->max_contrib));
+        if (stride > ws_stride) {
+            drop_graph();
+            ws_stride = stride;
+            ws_buffers = 0;
+            for (int nb = 8; nb >= 2 && !ws_buffers; nb--)
+                if (nb * ws_stride + 16 * (size_t)nb + 32 * (size_t)kWsGroups <= 227 * 1024) ws_buffers = nb;
+            ws_smem = ws_buffers ? ws_buffers * ws_stride + 16 * (size_t)ws_buffers + 32 * (size_t)kWsGroups : 0;
+        }
         if (!counts.p) counts.alloc(2);
         if (nm) {
             E3D_CUDA(cudaMemcpyAsync(args.p, A.data(), A.size() * sizeof(StageArgs), cudaMemcpyHostToDevice, stream));
@@ -162,7 +180,17 @@ struct Batch {
         dirty = false;
     }
 
-    void launch_stage(const BatchStage &bs) {
+    bool use_ws() const { return kernel == E3D_BATCH_KERNEL_WS && precision != E3D_PREC_FP32_FLUX && ws_buffers >= 2; }
+
+    void launch_stage(BatchStage bs) {
+        if (use_ws()) {
+            bs.ws_buffers = ws_buffers;
+            bs.ws_stride = (int)ws_stride;
+            const int grid = std::max(1, std::min(tile_cap, n_sm));
+            if (precision == E3D_PREC_FP64_EXACT) launch_batch_ws_exact(bs, grid, ws_smem, stream);
+            else launch_batch_ws_fast(bs, grid, ws_smem, stream);
+            return;
+        }
         if (precision == E3D_PREC_FP32_FLUX) launch_batch_f32(bs, tile_cap, smem_cap, stream);
         else if (precision == E3D_PREC_FP64_EXACT) launch_batch_exact(bs, tile_cap, smem_cap, stream);
         else launch_batch_fast(bs, tile_cap, smem_cap, stream);
@@ -172,9 +200,10 @@ struct Batch {
     // read-back, as one graph.
     void build_graph(int iters) {
         drop_graph();
-        if (precision == E3D_PREC_FP32_FLUX) prepare_batch_f32(smem_cap);
-        else if (precision == E3D_PREC_FP64_EXACT) prepare_batch_exact(smem_cap);
-        else prepare_batch_fast(smem_cap);
+        const size_t wss = use_ws() ? ws_smem : 0;
+        if (precision == E3D_PREC_FP32_FLUX) prepare_batch_f32(smem_cap, 0);
+        else if (precision == E3D_PREC_FP64_EXACT) prepare_batch_exact(smem_cap, wss);
+        else prepare_batch_fast(smem_cap, wss);
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
         cudaGraph_t g;
         E3D_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -309,6 +338,7 @@ e3d_status e3d_batch_create(int32_t device, void *stream, e3d_batch **out) {
             E3D_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
             B->own_stream = true;
         }
+        E3D_CUDA(cudaDeviceGetAttribute(&B->n_sm, cudaDevAttrMultiProcessorCount, device));
         E3D_CUDA(cudaEventCreate(&B->ev0));
         E3D_CUDA(cudaEventCreate(&B->ev1));
         E3D_CUDA(cudaMallocHost(&B->one_host, sizeof(int)));
@@ -408,6 +438,22 @@ e3d_status e3d_batch_remove(e3d_batch *batch, e3d_solver *solver, e3d_run_stats 
         B->release(B->members[k], stats);
         B->members.erase(B->members.begin() + k);
         B->dirty = true;
+    });
+}
+
+e3d_status e3d_batch_set_kernel(e3d_batch *batch, int32_t kernel) {
+    return guarded([&] {
+        if (!batch) throw Error(E3D_ERR_INVALID_ARG, "NULL argument");
+        if (kernel != E3D_BATCH_KERNEL_TILES && kernel != E3D_BATCH_KERNEL_WS)
+            throw Error(E3D_ERR_INVALID_ARG, "unknown batch stage kernel");
+        Batch *B = as_batch(batch);
+        std::lock_guard<std::mutex> lock(B->mu);
+        if (kernel != B->kernel) {
+            E3D_CUDA(cudaSetDevice(B->device));
+            E3D_CUDA(cudaStreamSynchronize(B->stream));
+            B->drop_graph();
+            B->kernel = kernel;
+        }
     });
 }
 

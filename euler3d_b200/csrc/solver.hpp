@@ -26,12 +26,14 @@ constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
 void launch_update_exact(const StageArgs &a, cudaStream_t s);
 void launch_update_fast(const StageArgs &a, cudaStream_t s);
-void prepare_batch_exact(size_t smem_bytes);
-void prepare_batch_fast(size_t smem_bytes);
-void prepare_batch_f32(size_t smem_bytes);
+void prepare_batch_exact(size_t smem_bytes, size_t ws_smem_bytes);
+void prepare_batch_fast(size_t smem_bytes, size_t ws_smem_bytes);
+void prepare_batch_f32(size_t smem_bytes, size_t ws_smem_bytes);
 void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+void launch_batch_ws_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+void launch_batch_ws_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 
 struct CoeffArgs {
     int n_wall;

@@ -939,6 +939,7 @@ struct BatchStage {
     const int *__restrict__ n_entries;   // valid table entries; later blocks return at once
     double alpha;
     int first_stage, last_stage, parity;
+    int ws_buffers, ws_stride;           // tile_ws_batch_kernel: buffers, bytes per buffer
 };
 static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied in 8-byte words");
 
@@ -986,6 +987,10 @@ __global__ void __launch_bounds__(kStageThreads, MINB) tile_batch_kernel(BatchSt
 constexpr int kWsGroups = 5;
 constexpr int kWsThreads = 32 + kWsGroups * kTileCells;
 
+// Bytes ahead of a batch buffer's tile data that hold the member's StageArgs.
+constexpr size_t kWsArgsSlot = (sizeof(StageArgs) + 127) & ~(size_t)127;
+static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is bulk-copied");
+
 __host__ __device__ __forceinline__ size_t ws_buffer_bytes(int LC, int FC, int MC) {
     return (tile_buf_bytes(LC, FC, MC) + 127) & ~(size_t)127;
 }
@@ -1021,16 +1026,33 @@ __device__ __forceinline__ void ws_halo_copy(const StageArgs &a, double2 *dst, i
     bulk_g2s(dst, a.qin + 3 * (size_t)h, 48u, bar);
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
-    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
-    const int B = a.ws_buffers, n_tiles = a.n_tiles, G = gridDim.x;
-    const size_t bb = ws_buffer_bytes(LC, FC, MC);
+// Body of the warp-specialised kernels.  Solo (BATCH false): work item k of the block is tile
+// blockIdx.x + k gridDim.x of the one solver whose arguments `solo` holds.  Batch (BATCH true): work
+// item k is entry blockIdx.x + k gridDim.x of the batch's (member, tile) table; the producer copies
+// the member's StageArgs into the buffer beside the tile's data, and the consumer group sets the
+// stage's alpha and flags in that copy before it reads it -- so each member computes what its solo
+// run computes.  A stopped member's items carry only the arguments, which the consumers skip.  A
+// wait that gives up sets the fault word of the member whose item it waited for.
+template <bool EXACT, bool BATCH>
+__device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage &bs, unsigned char *smem_raw) {
+    const int T = kTileCells, G = gridDim.x;
+    const int B = BATCH ? bs.ws_buffers : solo.ws_buffers;
+    const int n_items = BATCH ? *bs.n_entries : solo.n_tiles;
+    const size_t slot = BATCH ? kWsArgsSlot : 0;  // the member's arguments, ahead of the tile's data
+    const size_t bb = BATCH ? (size_t)bs.ws_stride : ws_buffer_bytes(solo.smem_cells, solo.smem_faces, solo.max_contrib);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)B * bb);
     uint64_t *empty = full + B;
     double *gsum = reinterpret_cast<double *>(empty + B);  // [kWsGroups][4]
+    // the arguments (in global memory, or the kernel's own) of work item `item`, and its tile
+    auto item_args = [&](int item, int &tile) -> const StageArgs * {
+        if (!BATCH) {
+            tile = item;
+            return &solo;
+        }
+        const int2 e = bs.table[item];
+        tile = e.y;
+        return bs.args + 2 * e.x + bs.parity;
+    };
     if (threadIdx.x == 0) {
         for (int k = 0; k < B; k++) {
             mbar_init(&full[k], 1);
@@ -1041,51 +1063,62 @@ __global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 0) {  // ------------------------------------------------ producer
-        int issued = 0;  // tiles whose copies were issued (buffer of tile k: k % B)
-        bool stop = false;
-        for (int k = 0, tile = blockIdx.x; tile < n_tiles && !stop; k++, tile += G) {
+        int issued = 0;  // items whose copies were issued (buffer of item k: k % B)
+        bool stopped = false;
+        for (int k = 0, item = blockIdx.x; item < n_items; k++, item += G) {
             const int bi = k % B;
-            if (k >= B) {  // the buffer's previous tile (k - B) has been handed back
+            if (k >= B) {  // the buffer's previous item (k - B) has been handed back
                 // lane 0 waits and the warp follows its answer, so every decision is warp-uniform
                 int ok = 0;
                 if (lane == 0) {
+                    int prev_tile;
+                    int *prev_fault = item_args(item - B * G, prev_tile)->fault;
                     const uint32_t par = (uint32_t)(((k / B) - 1) & 1);
                     for (int it = 0; it < kWaitLimit && !ok; it++) {
                         ok = mbar_try_wait(&empty[bi], par);
-                        if (!ok && (it & 255) == 255 && *(volatile int *)a.fault) break;
+                        if (!ok && (it & 255) == 255 && *(volatile int *)prev_fault) break;
                     }
-                    if (!ok) atomicExch(a.fault, 1);
+                    if (!ok) atomicExch(prev_fault, 1);
                 }
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                if (!ok) {
-                    stop = true;
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    stopped = true;
                     break;
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             }
-            const TileBuf b = tile_buf_at(smem_raw + (size_t)bi * bb, LC, FC, MC);
+            unsigned char *base = smem_raw + (size_t)bi * bb;
+            int tile;
+            const StageArgs &a = *item_args(item, tile);
+            const bool skip = BATCH && a.ctl->done;  // a stopped member: its arguments only
+            const TileBuf tb = tile_buf_at(base + slot, a.smem_cells, a.smem_faces, a.max_contrib);
             const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-            const int nh = a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
+            const int nh = skip ? 0 : a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
             if (lane == 0) {
-                const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
-                const uint32_t bytes = (uint32_t)nloc * 48u + round16(40u * (uint32_t)nf) + (uint32_t)MC * T * 2u +
-                                       (uint32_t)nh * 48u;
-                mbar_expect_tx(&full[bi], bytes);
-                bulk_g2s(b.st, a.qin + 3 * (size_t)c0, (uint32_t)nloc * 48u, &full[bi]);
-                bulk_g2s(b.rec, a.tile_rec + a.tile_rec_off[tile], round16(40u * (uint32_t)nf), &full[bi]);
-                bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, (uint32_t)MC * T * 2u, &full[bi]);
-                const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
-                for (int q = 0; q < 5; q++) bulk_prefetch_l2(a.w0 + (size_t)q * a.w0_stride + c0, b_w0);
-                bulk_prefetch_l2(a.cgeo + c0, (uint32_t)nloc * 32u);
+                const int nf = skip ? 0 : a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+                const uint32_t b_ct = (uint32_t)a.max_contrib * T * 2u;
+                const uint32_t tile_bytes =
+                    skip ? 0u : (uint32_t)nloc * 48u + round16(40u * (uint32_t)nf) + b_ct + (uint32_t)nh * 48u;
+                mbar_expect_tx(&full[bi], tile_bytes + (BATCH ? (uint32_t)sizeof(StageArgs) : 0u));
+                if (BATCH) bulk_g2s(base, &a, (uint32_t)sizeof(StageArgs), &full[bi]);
+                if (!skip) {
+                    bulk_g2s(tb.st, a.qin + 3 * (size_t)c0, (uint32_t)nloc * 48u, &full[bi]);
+                    bulk_g2s(tb.rec, a.tile_rec + a.tile_rec_off[tile], round16(40u * (uint32_t)nf), &full[bi]);
+                    bulk_g2s(tb.ct, a.tile_contrib + (size_t)tile * a.max_contrib * T, b_ct, &full[bi]);
+                    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
+                    for (int q = 0; q < 5; q++) bulk_prefetch_l2(a.w0 + (size_t)q * a.w0_stride + c0, b_w0);
+                    bulk_prefetch_l2(a.cgeo + c0, (uint32_t)nloc * 32u);
+                }
             }
             __syncwarp();  // the expected byte count is posted before any halo copy can complete
-            const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
-            for (int i = lane; i < nh; i += 32) ws_halo_copy(a, b.st + 3 * (nloc + i), hrow[i], &full[bi]);
+            if (!skip) {
+                const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+                for (int i = lane; i < nh; i += 32) ws_halo_copy(a, tb.st + 3 * (nloc + i), hrow[i], &full[bi]);
+            }
             issued = k + 1;
         }
-        // every copy issued must land before the block can leave (the consumers normally wait for
-        // them; after a fault they may not have)
-        if (lane == 0 && *(volatile int *)a.fault) {
+        // every copy issued must land before the block can leave (the consumers wait for them when
+        // the walk completes; after a give-up they may not have)
+        if (lane == 0 && stopped) {
             for (int k = (issued > B ? issued - B : 0); k < issued; k++)
                 tile_drain(&full[k % B], (uint32_t)((k / B) & 1));
         }
@@ -1093,38 +1126,71 @@ __global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
     }
 
     // ------------------------------------------------------------------ consumer group
-    const int grp = warp - 1 >= 0 ? (threadIdx.x - 32) / T : 0;
+    const int grp = (threadIdx.x - 32) / T;
     const int tid = (threadIdx.x - 32) % T;
     const int bar_id = 1 + grp;
     double *fsum = gsum + 4 * grp;
-    for (int k = grp, tile = blockIdx.x + grp * G; tile < n_tiles; k += kWsGroups, tile += kWsGroups * G) {
+    for (int k = grp, item = blockIdx.x + grp * G; item < n_items; k += kWsGroups, item += kWsGroups * G) {
         const int bi = k % B;
+        unsigned char *base = smem_raw + (size_t)bi * bb;
+        int tile;
+        const StageArgs *ag = item_args(item, tile);  // global (batch) or the kernel's own arguments
         bool ok = false;
-        for (int it = 0; it < a.wait_polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)((k / B) & 1));
-        if (!ok) atomicExch(a.fault, 1);
+        const int polls = ag->wait_polls;
+        for (int it = 0; it < polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)((k / B) & 1));
+        if (!ok) atomicExch(ag->fault, 1);
+        if (BATCH && ok && tid == 0) {  // this stage's alpha and flags in the member's arguments
+            StageArgs *sa = reinterpret_cast<StageArgs *>(base);
+            sa->alpha = bs.alpha;
+            sa->first_stage = bs.first_stage;
+            sa->last_stage = bs.last_stage;
+            sa->residual_only = 0;
+        }
         if (named_sync_or(bar_id, T, !ok)) return;  // the same decision for the whole group
-        const TileBuf b = tile_buf_at(smem_raw + (size_t)bi * bb, LC, FC, MC);
-        const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-        const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
-        double *fs = reinterpret_cast<double *>(b.rec);
-        tile_fluxes<EXACT, kTileCells>(a, b, fs, nf, c0, tid);
-        double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (tid < nloc) tile_load_cell(a, c0, tid, W0, cg);
-        named_sync(bar_id, T);
+        const StageArgs &a = BATCH ? *reinterpret_cast<const StageArgs *>(base) : solo;
+        const bool run = !BATCH || !a.ctl->done;  // the member of a batch item may have stopped
         double r2 = 0.0;
-        if (tid < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, tid, W0, cg);
-        named_sync(bar_id, T);  // every read of the buffer is done
-        if (tid == 0) mbar_arrive(&empty[bi]);
-        if (a.last_stage && !a.residual_only) {
+        if (run) {
+            const TileBuf b = tile_buf_at(base + slot, a.smem_cells, a.smem_faces, a.max_contrib);
+            const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
+            const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+            double *fs = reinterpret_cast<double *>(b.rec);
+            tile_fluxes<EXACT, kTileCells>(a, b, fs, nf, c0, tid);
+            double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (tid < nloc) tile_load_cell(a, c0, tid, W0, cg);
+            named_sync(bar_id, T);
+            if (tid < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, tid, W0, cg);
+        }
+        const bool sum = run && a.last_stage && !a.residual_only;  // uniform across the group
+        double *partial = sum ? a.partials + tile : nullptr;
+        if (sum) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
             if ((tid & 31) == 0) fsum[tid >> 5] = r2;
-            named_sync(bar_id, T);
-            if (tid == 0) a.partials[tile] = (fsum[0] + fsum[1]) + (fsum[2] + fsum[3]);
-            named_sync(bar_id, T);  // fsum is reused by the next tile
         }
+        named_sync(bar_id, T);  // every read of the buffer (the arguments included) is done
+        if (tid == 0) {
+            // the order of block_sum_store's last shuffle tree, so every kernel writes the same partial
+            if (sum) *partial = (fsum[0] + fsum[2]) + (fsum[1] + fsum[3]);
+            mbar_arrive(&empty[bi]);
+        }
+        if (sum) named_sync(bar_id, T);  // fsum is reused by the next item
     }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ws_body<EXACT, false>(a, BatchStage{}, smem_raw);
+}
+
+// Several solvers in one persistent grid: the batch's (member, tile) table walked as above.
+template <bool EXACT>
+__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_batch_kernel(BatchStage bs) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ws_body<EXACT, true>(StageArgs{}, bs, smem_raw);
 }
 
 // ---- update phase of a split stage

@@ -9,7 +9,7 @@ void prepare_tile_f32(size_t smem_bytes) {
     raise_smem_limit((const void *)tile_kernel_f32<8>, smem_bytes);
 }
 
-void prepare_batch_f32(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel_f32<7>, smem_bytes); }
+void prepare_batch_f32(size_t smem_bytes, size_t) { raise_smem_limit((const void *)tile_batch_kernel_f32<7>, smem_bytes); }
 
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {

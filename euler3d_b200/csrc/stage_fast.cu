@@ -12,7 +12,10 @@ void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<false>, pipe_smem_bytes);
 }
 
-void prepare_batch_fast(size_t smem_bytes) { raise_smem_limit((const void *)tile_batch_kernel<false, 6>, smem_bytes); }
+void prepare_batch_fast(size_t smem_bytes, size_t ws_smem_bytes) {
+    raise_smem_limit((const void *)tile_batch_kernel<false, 6>, smem_bytes);
+    if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<false>, ws_smem_bytes);
+}
 
 // Update phase of a split stage (residual smoothing between residual and update).
 void launch_update_fast(const StageArgs &a, cudaStream_t s) {
@@ -22,6 +25,11 @@ void launch_update_fast(const StageArgs &a, cudaStream_t s) {
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
     tile_batch_kernel<false, 6><<<grid, kStageThreads, smem_bytes, s>>>(bs);
+}
+
+// The same stage with the warp-specialised persistent kernel: `grid` blocks walk the table.
+void launch_batch_ws_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
+    tile_ws_batch_kernel<false><<<grid, kWsThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;

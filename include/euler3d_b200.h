@@ -351,6 +351,16 @@ e3d_status e3d_batch_retire(e3d_batch *batch, e3d_solver **solvers, e3d_run_stat
 /* Takes `solver` out of the batch whether or not its run has stopped; stats as e3d_batch_retire. */
 e3d_status e3d_batch_remove(e3d_batch *batch, e3d_solver *solver, e3d_run_stats *stats);
 
+/* The stage kernel of a batch's launches (FP64 and FP64_EXACT batches; an FP32_FLUX batch always
+ * runs the first):
+ *   E3D_BATCH_KERNEL_TILES  one block of 128 threads per (member, tile) entry of the table (default)
+ *   E3D_BATCH_KERNEL_WS     one persistent block per SM walking the table: a producer warp copies each
+ *                           entry's member arguments and tile data into a ring of shared-memory buffers
+ *                           ahead of five consumer groups that evaluate them
+ * Both compute the same bits.  No counterpart in the reference. */
+enum { E3D_BATCH_KERNEL_TILES = 0, E3D_BATCH_KERNEL_WS = 1 };
+e3d_status e3d_batch_set_kernel(e3d_batch *batch, int32_t kernel);
+
 typedef struct e3d_batch_info {
 	int32_t n_members;                /* members (running or stopped, not yet retired) */
 	int32_t n_running;                /* members whose runs have not stopped */

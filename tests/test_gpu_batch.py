@@ -60,10 +60,12 @@ def collect(solver, stats):
     return solver.get_state(), solver.rms_history(), stats
 
 
-@pytest.mark.parametrize("precision", PRECISIONS)
-def test_mix_equals_alone(precision):
+@pytest.mark.parametrize("precision,kernel", [(p, _lib.BATCH_KERNEL_TILES) for p in PRECISIONS] +
+                         [(_lib.PREC_FP64_EXACT, _lib.BATCH_KERNEL_WS), (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+def test_mix_equals_alone(precision, kernel):
     refs = [alone(n, sc, sd, precision, rp) for n, sc, sd, rp in MIX]
     b = Batch()
+    b.set_kernel(kernel)
     solvers = []
     for n, sc, sd, rp in MIX:
         s = make_solver(n, sc, sd, precision)
@@ -81,11 +83,14 @@ def test_mix_equals_alone(precision):
     b.close()
 
 
-@pytest.mark.parametrize("precision", [_lib.PREC_FP64, _lib.PREC_FP32_FLUX])
-def test_staggered_admission(precision):
+@pytest.mark.parametrize("precision,kernel", [(_lib.PREC_FP64, _lib.BATCH_KERNEL_TILES),
+                                              (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_TILES),
+                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+def test_staggered_admission(precision, kernel):
     """Members join a running batch between steps (continuous admission) and leave as they stop."""
     refs = [alone(n, sc, sd, precision, rp) for n, sc, sd, rp in MIX]
     b = Batch()
+    b.set_kernel(kernel)
     solvers, results = [], {}
     for i, (n, sc, sd, rp) in enumerate(MIX):
         s = make_solver(n, sc, sd, precision)

@@ -80,8 +80,10 @@ def test_timeout_stops_run_and_solver_recovers(precision, kernel):
             assert np.array_equal(g[k], r[k]), k
 
 
-@pytest.mark.parametrize("precision", [_lib.PREC_FP64, _lib.PREC_FP32_FLUX])
-def test_timeout_in_batch_member(precision):
+@pytest.mark.parametrize("precision,kernel", [(_lib.PREC_FP64, _lib.BATCH_KERNEL_TILES),
+                                              (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_TILES),
+                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+def test_timeout_in_batch_member(precision, kernel):
     """A member whose waits give up is retired with E3D_ERR_TIMEOUT; the member beside it is not
     disturbed (it equals its run alone bit for bit), and the timed-out solver runs normally once
     it is handed back."""
@@ -94,6 +96,7 @@ def test_timeout_in_batch_member(precision):
     alone_stats = alone.run(40, sampling=4, stage_kernel=_lib.KERNEL_TILE)
     bad.set_wait_limit(0)
     b = Batch()
+    b.set_kernel(kernel)
     b.add(bad, 40, sampling=4)
     b.add(good, 40, sampling=4)
     done = {id(s): (stats, status) for s, stats, status in b.run_all(8)}
