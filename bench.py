@@ -48,8 +48,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "fp64_exact", "fp32"], default="fp64")
     ap.add_argument("--ordering", choices=["spatial", "rcm", "native"], default="spatial")
     ap.add_argument("--kernel", type=int, default=0,
-                    help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 warp-specialised persistent face tiles, 5 face tiles at 7 blocks/SM "
-                         "(FP32_FLUX: 3 and 4 are its two face-tile register budgets)")
+                    help="stage kernel: 0 autotuned, 1/2 gather, 3 face tiles, 4 warp-specialised persistent face tiles, "
+                         "5 face tiles at 7 blocks/SM (FP32_FLUX: 8 blocks/SM)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--mode", choices=["all", "stage", "served", "profile", "kernels"], default="all",
@@ -345,9 +345,9 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_kernel_f32<8>"] if args.precision == "fp32" else
+                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_ws_kernel<WS_F32>", "tile_kernel_f32<8>"] if args.precision == "fp32" else
                                 ["stage_kernel<false,4>", "stage_kernel<false,5>", "tile_kernel<false,4>",
-                                 "tile_ws_kernel<false>", "tile_kernel<false,7>"])[solver.info()["stage_variant"]],
+                                 "tile_ws_kernel<WS_FAST>", "tile_kernel<false,7>"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "launches_timed": tstats["stage_launches"],
                      "timing": "event pairs around every stage kernel in a second run of the timed graph",

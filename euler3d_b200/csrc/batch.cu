@@ -21,7 +21,7 @@
 #include <vector>
 
 #include "solver.hpp"
-#include "stage_f32.cuh"
+#include "stage_ws.cuh"
 
 namespace e3d {
 
@@ -55,7 +55,7 @@ struct Batch {
     int member_cap = 0, tile_cap = 0;
     size_t smem_cap = 0;
     // stage kernel: E3D_BATCH_KERNEL_TILES (one block per table entry) or E3D_BATCH_KERNEL_WS (the
-    // warp-specialised persistent kernel walking the table, FP64 modes); its ring of buffers
+    // warp-specialised persistent kernel walking the table); its ring of buffers
     int kernel = E3D_BATCH_KERNEL_TILES;
     int n_sm = 0;
     int ws_buffers = 0;
@@ -154,15 +154,15 @@ struct Batch {
         }
         // the warp-specialised kernel's buffers: the largest member's tile data plus its arguments
         size_t stride = 0;
-        for (const Member &m : members)
-            stride = std::max(stride, kWsArgsSlot + ws_buffer_bytes(m.S->smem_cells, m.S->smem_faces, m.S->max_contrib));
+        for (const Member &m : members) {
+            const int wp = m.S->f32 ? WS_F32 : m.S->prm.precision == E3D_PREC_FP64 ? WS_FAST : WS_EXACT;
+            stride = std::max(stride, kWsArgsSlot + ws_buffer_bytes(wp, m.S->smem_cells, m.S->smem_faces, m.S->max_contrib));
+        }
         if (stride > ws_stride) {
             drop_graph();
             ws_stride = stride;
-            ws_buffers = 0;
-            for (int nb = 8; nb >= 2 && !ws_buffers; nb--)
-                if (nb * ws_stride + 16 * (size_t)nb + 32 * (size_t)kWsGroups <= 227 * 1024) ws_buffers = nb;
-            ws_smem = ws_buffers ? ws_buffers * ws_stride + 16 * (size_t)ws_buffers + 32 * (size_t)kWsGroups : 0;
+            ws_buffers = ws_buffers_for(ws_stride);
+            ws_smem = ws_buffers ? ws_smem_for(ws_stride, ws_buffers) : 0;
         }
         if (!counts.p) counts.alloc(2);
         if (nm) {
@@ -180,14 +180,15 @@ struct Batch {
         dirty = false;
     }
 
-    bool use_ws() const { return kernel == E3D_BATCH_KERNEL_WS && precision != E3D_PREC_FP32_FLUX && ws_buffers >= 2; }
+    bool use_ws() const { return kernel == E3D_BATCH_KERNEL_WS && ws_buffers >= 2; }
 
     void launch_stage(BatchStage bs) {
         if (use_ws()) {
             bs.ws_buffers = ws_buffers;
             bs.ws_stride = (int)ws_stride;
             const int grid = std::max(1, std::min(tile_cap, n_sm));
-            if (precision == E3D_PREC_FP64_EXACT) launch_batch_ws_exact(bs, grid, ws_smem, stream);
+            if (precision == E3D_PREC_FP32_FLUX) launch_batch_ws_f32(bs, grid, ws_smem, stream);
+            else if (precision == E3D_PREC_FP64_EXACT) launch_batch_ws_exact(bs, grid, ws_smem, stream);
             else launch_batch_ws_fast(bs, grid, ws_smem, stream);
             return;
         }
@@ -201,7 +202,7 @@ struct Batch {
     void build_graph(int iters) {
         drop_graph();
         const size_t wss = use_ws() ? ws_smem : 0;
-        if (precision == E3D_PREC_FP32_FLUX) prepare_batch_f32(smem_cap, 0);
+        if (precision == E3D_PREC_FP32_FLUX) prepare_batch_f32(smem_cap, wss);
         else if (precision == E3D_PREC_FP64_EXACT) prepare_batch_exact(smem_cap, wss);
         else prepare_batch_fast(smem_cap, wss);
         static const double alphas[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};

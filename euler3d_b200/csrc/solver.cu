@@ -16,7 +16,7 @@
 #include "common.hpp"
 #include "euler3d_b200.h"
 #include "solver.hpp"
-#include "stage_f32.cuh"
+#include "stage_ws.cuh"
 
 namespace e3d {
 
@@ -665,11 +665,11 @@ static void build_tiles(Solver *S, const std::vector<int> &cptr, const std::vect
     int max_halo = 0;
     for (int t = 0; t < n_tiles; t++) max_halo = std::max(max_halo, halo_ptr[t + 1] - halo_ptr[t]);
     // the warp-specialised kernel's ring: as many tile buffers as fit (at most eight, at least two)
-    S->ws_buffers = 0;
-    for (int nb = 8; nb >= 2 && !S->ws_buffers; nb--)
-        if (ws_smem_bytes(max_cells, max_faces, max_contrib, nb) <= 227 * 1024) S->ws_buffers = nb;
+    const int ws_prec = S->prm.precision == E3D_PREC_FP32_FLUX ? WS_F32 : S->prm.precision == E3D_PREC_FP64 ? WS_FAST : WS_EXACT;
+    const size_t ws_stride = ws_buffer_bytes(ws_prec, max_cells, max_faces, max_contrib);
+    S->ws_buffers = ws_buffers_for(ws_stride);
     S->pipe_ok = ok && S->ws_buffers >= 2;
-    S->pipe_smem = S->pipe_ok ? ws_smem_bytes(max_cells, max_faces, max_contrib, S->ws_buffers) : 0;
+    S->pipe_smem = S->pipe_ok ? ws_smem_for(ws_stride, S->ws_buffers) : 0;
     if (!S->tiles_ok) return;
     cudaStream_t s = S->stream;
     // halo lists at a fixed stride per tile, padded with -1: a block reads its entries without
@@ -1291,7 +1291,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
             const int v = rp->stage_kernel - 1;
             if (!S->variant_ok(v))
                 throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh and precision");
-            if (S->f32) prepare_tile_f32(S->tile32_smem);
+            if (S->f32) prepare_tile_f32(S->tile32_smem, S->pipe_smem);
             else if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);
             else if (v >= 2) prepare_tile_fast(S->tile_smem, S->pipe_smem);
             if (v != S->variant && S->graph) {

@@ -18,7 +18,7 @@ void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
 void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
-void prepare_tile_f32(size_t smem_bytes);
+void prepare_tile_f32(size_t smem_bytes, size_t ws_smem_bytes);
 // gather (two register budgets), face tiles, warp-specialised persistent face tiles, face tiles at 7 blocks/SM
 constexpr int kStageVariants = 5;
 
@@ -34,6 +34,7 @@ void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaSt
 void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 void launch_batch_ws_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 void launch_batch_ws_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
+void launch_batch_ws_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s);
 
 struct CoeffArgs {
     int n_wall;
@@ -278,11 +279,11 @@ struct Solver {
     float variant_ms[kStageVariants] = {};
 
     // Variants compiled for this precision and possible on this mesh.  FP32_FLUX mode has face-tile
-    // kernels only (variants 2 and 3 are its two register budgets); the seven-blocks-per-SM face-tile
-    // kernel exists for FP64 only (in FP64_EXACT it would spill).
+    // kernels only (2 and 4 are its two register budgets, 3 the warp-specialised one); variant 4 is
+    // the seven-blocks-per-SM face-tile kernel in FP64 (in FP64_EXACT it would spill).
     bool variant_ok(int v) const {
         if (v < 0 || v >= kStageVariants) return false;
-        if (f32) return v == 2 || v == 3;
+        if (f32) return v == 2 || v == 4 || (v == 3 && pipe_ok);
         if (v == 2) return tiles_ok;
         if (v == 3) return pipe_ok;
         if (v == 4) return tiles_ok && prm.precision == E3D_PREC_FP64;
@@ -309,7 +310,7 @@ struct Solver {
         const int reps = N > 200000 ? 3 : 10;
         float best = 1e30f;
         if (f32) {
-            prepare_tile_f32(tile32_smem);
+            prepare_tile_f32(tile32_smem, pipe_smem);
         } else if (tiles_ok) {
             if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
             else prepare_tile_fast(tile_smem, pipe_smem);
@@ -339,8 +340,8 @@ struct Solver {
     void use_default_variant() {
         for (auto &m : variant_ms) m = -1.0f;
         if (f32) {
-            variant = 3;
-            prepare_tile_f32(tile32_smem);
+            variant = 4;
+            prepare_tile_f32(tile32_smem, pipe_smem);
         } else if (tiles_ok) {
             variant = prm.precision == E3D_PREC_FP64 ? 4 : 2;
             if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);

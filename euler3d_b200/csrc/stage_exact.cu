@@ -1,19 +1,19 @@
 // FP64_EXACT instantiations of the stage kernels.  Built with -fmad=false so that every double
 // operation rounds exactly as the reference's source order does.
 #include "common.hpp"
-#include "stage.cuh"
+#include "stage_ws.cuh"
 
 namespace e3d {
 
 // Dynamic shared memory the tile kernels may use (raised before their first launch).
 void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes) {
     raise_smem_limit((const void *)tile_kernel<true, 4>, smem_bytes);
-    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<true>, pipe_smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<WS_EXACT>, pipe_smem_bytes);
 }
 
 void prepare_batch_exact(size_t smem_bytes, size_t ws_smem_bytes) {
     raise_smem_limit((const void *)tile_batch_kernel<true, 4>, smem_bytes);
-    if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<true>, ws_smem_bytes);
+    if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<WS_EXACT>, ws_smem_bytes);
 }
 
 // Update phase of a split stage (residual smoothing between residual and update).
@@ -28,7 +28,7 @@ void launch_batch_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaS
 
 // The same stage with the warp-specialised persistent kernel: `grid` blocks walk the table.
 void launch_batch_ws_exact(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_ws_batch_kernel<true><<<grid, kWsThreads, smem_bytes, s>>>(bs);
+    tile_ws_batch_kernel<WS_EXACT><<<grid, kWsThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, registers for 2 blocks/SM; 1: gather kernel, 4 blocks/SM;
@@ -36,8 +36,8 @@ void launch_batch_ws_exact(const BatchStage &bs, int grid, size_t smem_bytes, cu
 void launch_stage_exact(const StageArgs &a, cudaStream_t s, int variant) {
     const int blocks = (a.n_cells + kStageThreads - 1) / kStageThreads;
     if (variant == 3) {
-        const size_t smem = ws_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, a.ws_buffers);
-        tile_ws_kernel<true><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
+        const size_t smem = ws_smem_for(ws_buffer_bytes(WS_EXACT, a.smem_cells, a.smem_faces, a.max_contrib), a.ws_buffers);
+        tile_ws_kernel<WS_EXACT><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<true, 4><<<blocks, kStageThreads, smem, s>>>(a);

@@ -117,84 +117,43 @@ __device__ __forceinline__ PrimF prim32(const float4 *st, int i) {
 // face j are written over its 24-byte record (fs[6 j + k]), which only the thread evaluating the
 // face reads.  W0 and the cell geometry stay in global memory (prefetched into L2 when the tile
 // starts, read into registers before the flux phase ends), as in tile_body.
+struct Tile32 {
+    float4 *st;
+    FaceRec32 *rec;
+    unsigned short *ct;
+};
+
+__host__ __device__ __forceinline__ size_t tile32_buf_bytes(int LC, int FC, int MC) {
+    return (size_t)LC * 32 + ((24u * (size_t)FC + 15) & ~(size_t)15) + (size_t)MC * kTileCells * 2;
+}
+
+__device__ __forceinline__ Tile32 tile32_at(unsigned char *base, int LC, int FC) {
+    Tile32 b;
+    b.st = reinterpret_cast<float4 *>(base);
+    b.rec = reinterpret_cast<FaceRec32 *>(base + (size_t)LC * 32);
+    b.ct = reinterpret_cast<unsigned short *>(base + (size_t)LC * 32 + round16(24u * FC));
+    return b;
+}
+
 inline size_t tile32_smem_bytes(int smem_cells, int smem_faces, int max_contrib) {
-    size_t b = (size_t)smem_cells * 32 + ((24u * (size_t)smem_faces + 15) & ~(size_t)15) +
-               (size_t)max_contrib * kTileCells * 2;
-    b = (b + 15) & ~(size_t)15;
+    const size_t b = (tile32_buf_bytes(smem_cells, smem_faces, max_contrib) + 15) & ~(size_t)15;
     return b + 16;
 }
 
-// Body shared by tile_kernel_f32 (one solver) and tile_batch_kernel_f32 (several solvers in one
-// grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
-__device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, double *partial, unsigned char *smem_raw) {
-    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
-    size_t off = 0;
-    float4 *st = reinterpret_cast<float4 *>(smem_raw + off);
-    off += (size_t)LC * 32;
-    FaceRec32 *rec = reinterpret_cast<FaceRec32 *>(smem_raw + off);
-    off += round16(24u * FC);
-    unsigned short *cts = reinterpret_cast<unsigned short *>(smem_raw + off);
-    off += (size_t)MC * T * 2;
-    off = (off + 15) & ~(size_t)15;
-    float *fs = reinterpret_cast<float *>(rec);
-    off = (off + 15) & ~(size_t)15;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
-    const int c0 = tile * T;
-    const int nloc = min(T, a.n_cells - c0);
-    // independent loads first, as in tile_body
-    const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
-    const int i0 = threadIdx.x, i1 = threadIdx.x + T;
-    const int hx0 = i0 < a.halo_stride ? hrow[i0] : -1;
-    const int hx1 = i1 < a.halo_stride ? hrow[i1] : -1;
-    const int fp0 = a.tile_face_ptr[tile], fp1 = a.tile_face_ptr[tile + 1];
-    const long long rec_off = a.tile_rec32_off[tile];
-    const bool done = !a.residual_only && a.ctl->done;
-    const int nf = fp1 - fp0;
+// One flux per tile face, threads tid, tid + nt, ...; F*S of face j replaces record j.
+__device__ __forceinline__ void tile_fluxes_f32(const StageArgs &a, const Tile32 &b, int nf, int c0, int tid, int nt) {
     const float gf = (float)a.gamma;
-
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
-    if (done) return;  // uniform across the block
-    if (threadIdx.x == 0) {
-        const uint32_t b_state = (uint32_t)nloc * 32u;
-        const uint32_t b_rec = round16(24u * (uint32_t)nf);
-        const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
-        const uint32_t b_cg = (uint32_t)nloc * 16u;
-        const uint32_t b_ct = (uint32_t)MC * T * 2u;
-        mbar_expect_tx(bar, b_state + b_rec + b_ct);
-        bulk_g2s(st, a.q32in + 2 * (size_t)c0, b_state, bar);
-        bulk_g2s(rec, a.tile_rec32 + rec_off, b_rec, bar);
-        bulk_g2s(cts, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
-        for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
-        bulk_prefetch_l2(a.cgeo32 + c0, b_cg);
-    }
-    auto gather = [&](int i, int h) {
-        cp_async16(st + 2 * (nloc + i), a.q32in + 2 * (size_t)h);
-        cp_async16(st + 2 * (nloc + i) + 1, a.q32in + 2 * (size_t)h + 1);
-    };
-    if (hx0 >= 0) gather(i0, hx0);
-    if (hx1 >= 0) gather(i1, hx1);
-    for (int i = threadIdx.x + 2 * T; i < a.halo_stride; i += T) {
-        const int h = hrow[i];
-        if (h >= 0) gather(i, h);
-    }
-    cp_async_wait_all();
-    if (!tile_wait(a, bar, 0)) {
-        tile_drain(bar, 0);
-        return;
-    }
-
-    // one flux per tile face
-    for (int j = threadIdx.x; j < nf; j += kStageThreads) {
-        const FaceRec32 fr = rec[j];
+    float *fs = reinterpret_cast<float *>(b.rec);
+    for (int j = tid; j < nf; j += nt) {
+        const FaceRec32 fr = b.rec[j];
         const int l = fr.code & ((1 << kTileLocalBits) - 1);
         const int r = (fr.code >> kTileLocalBits) & ((1 << kTileLocalBits) - 1);
         const int tag = fr.code >> (2 * kTileLocalBits);
-        const PrimF L = prim32(st, l);
+        const PrimF L = prim32(b.st, l);
         float F[5];
         if (tag == TAG_LEFT) {
-            if (a.scheme == 1) ausm_f32(L, prim32(st, r), fr.nx, fr.ny, fr.nz, gf, F);
-            else roe_f32(L, prim32(st, r), fr.nx, fr.ny, fr.nz, gf, F);
+            if (a.scheme == 1) ausm_f32(L, prim32(b.st, r), fr.nx, fr.ny, fr.nz, gf, F);
+            else roe_f32(L, prim32(b.st, r), fr.nx, fr.ny, fr.nz, gf, F);
         } else {  // ghost cells are kept in double; their update uses the double boundary code
             const Prim Ld{L.rho, L.u, L.v, L.w, L.p, L.H};
             const double4 fg = make_double4(fr.nx, fr.ny, fr.nz, fr.S);
@@ -214,60 +173,122 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
 #pragma unroll
         for (int k = 0; k < 5; k++) fs[6 * j + k] = F[k] * fr.S;
     }
+}
+
+// The owner's W0 and geometry (global memory, prefetched into L2 when the tile started).
+__device__ __forceinline__ void tile_load_cell_f32(const StageArgs &a, int c, double W0[5], float4 &cg) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c];
+    cg = a.cgeo32[c];
+}
+
+// Cell i of the tile: sum of its faces' F*S, time step and update; returns R_rho^2 on the last stage.
+__device__ __forceinline__ double tile_update_f32(const StageArgs &a, const Tile32 &b, int c0, int i, const double W0[5],
+                                                  const float4 &cg) {
+    const int T = kTileCells, MC = a.max_contrib;
+    const float gf = (float)a.gamma;
+    const float *fs = reinterpret_cast<const float *>(b.rec);
+    const PrimF me = prim32(b.st, i);
+    double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    unsigned short e[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) e[k] = k < MC ? b.ct[k * T + i] : kNoContrib;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        if (e[k] == kNoContrib) break;
+        const int j = e[k] >> 1;
+        const double sg = (e[k] & 1) ? -1.0 : 1.0;  // fma by -/+1: the bits of R -/+ F*S (see tile_update)
+#pragma unroll
+        for (int q = 0; q < 5; q++) R[q] = fma(sg, (double)fs[6 * j + q], R[q]);
+    }
+    // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
+    const float snd = gf * me.p * me.r;
+    const float lam = 0.5f * fmaf(fabsf(me.u) + snd, cg.x, fmaf(fabsf(me.v) + snd, cg.y, (fabsf(me.w) + snd) * cg.z));
+    const int c = c0 + i;
+    if (a.residual_only) {
+        const int o = a.new2old[c];
+#pragma unroll
+        for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
+        a.dt_out[o] = (double)(a.cfl * cg.w / lam);
+        return 0.0;
+    }
+    // W = W0 - alpha dt R / V in double (alpha dt / V = alpha cfl / lambda)
+    const double coef = a.alpha * a.cfl * rcp_nr((double)lam);
+    double W[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) W[k] = fma(-coef, R[k], W0[k]);
+    const double ir = rcp_nr(W[0]);
+    const double u = W[1] * ir, v = W[2] * ir, w = W[3] * ir;
+    const double p = (a.gamma - 1.0) * fma(-0.5, fma(W[1], u, fma(W[2], v, W[3] * w)), W[4]);
+    const double H = (W[4] + p) * ir;
+    make_rec32(a.q32out + 2 * (size_t)c, W[0], u, v, w, p, H, a.gamma);
+    if (!a.last_stage) return 0.0;
+    // the conservative state carries over exactly in double
+    const size_t sd = (size_t)a.w0_stride;
+#pragma unroll
+    for (int k = 0; k < 5; k++) a.w0[k * sd + c] = W[k];
+    a.ecell[c] = W[4] * ir;
+    return R[0] * R[0];
+}
+
+// Body shared by tile_kernel_f32 (one solver) and tile_batch_kernel_f32 (several solvers in one
+// grid): `tile` is the solver's own tile index, `partial` where its RMS partial goes.
+__device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, double *partial, unsigned char *smem_raw) {
+    const int LC = a.smem_cells, FC = a.smem_faces, MC = a.max_contrib, T = kTileCells;
+    const Tile32 b = tile32_at(smem_raw, LC, FC);
+    const size_t off = (tile32_buf_bytes(LC, FC, MC) + 15) & ~(size_t)15;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + off);
+    const int c0 = tile * T;
+    const int nloc = min(T, a.n_cells - c0);
+    // independent loads first, as in tile_body
+    const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+    const int i0 = threadIdx.x, i1 = threadIdx.x + T;
+    const int hx0 = i0 < a.halo_stride ? hrow[i0] : -1;
+    const int hx1 = i1 < a.halo_stride ? hrow[i1] : -1;
+    const int fp0 = a.tile_face_ptr[tile], fp1 = a.tile_face_ptr[tile + 1];
+    const long long rec_off = a.tile_rec32_off[tile];
+    const bool done = !a.residual_only && a.ctl->done;
+    const int nf = fp1 - fp0;
+
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (done) return;  // uniform across the block
+    if (threadIdx.x == 0) {
+        const uint32_t b_state = (uint32_t)nloc * 32u;
+        const uint32_t b_rec = round16(24u * (uint32_t)nf);
+        const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
+        const uint32_t b_cg = (uint32_t)nloc * 16u;
+        const uint32_t b_ct = (uint32_t)MC * T * 2u;
+        mbar_expect_tx(bar, b_state + b_rec + b_ct);
+        bulk_g2s(b.st, a.q32in + 2 * (size_t)c0, b_state, bar);
+        bulk_g2s(b.rec, a.tile_rec32 + rec_off, b_rec, bar);
+        bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+        for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
+        bulk_prefetch_l2(a.cgeo32 + c0, b_cg);
+    }
+    auto gather = [&](int i, int h) {
+        cp_async16(b.st + 2 * (nloc + i), a.q32in + 2 * (size_t)h);
+        cp_async16(b.st + 2 * (nloc + i) + 1, a.q32in + 2 * (size_t)h + 1);
+    };
+    if (hx0 >= 0) gather(i0, hx0);
+    if (hx1 >= 0) gather(i1, hx1);
+    for (int i = threadIdx.x + 2 * T; i < a.halo_stride; i += T) {
+        const int h = hrow[i];
+        if (h >= 0) gather(i, h);
+    }
+    cp_async_wait_all();
+    if (!tile_wait(a, bar, 0)) {
+        tile_drain(bar, 0);
+        return;
+    }
+    tile_fluxes_f32(a, b, nf, c0, threadIdx.x, kStageThreads);
     const int i = threadIdx.x;
     double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     float4 cg = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (i < nloc) {  // the owner's W0 and geometry: their latency overlaps the barrier's wait
-#pragma unroll
-        for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
-        cg = a.cgeo32[c0 + i];
-    }
+    if (i < nloc) tile_load_cell_f32(a, c0 + i, W0, cg);  // latency overlaps the barrier's wait
     __syncthreads();
-
     double r2 = 0.0;
-    if (i < nloc) {
-        const PrimF me = prim32(st, i);
-        double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        unsigned short e[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) e[k] = k < MC ? cts[k * T + i] : kNoContrib;
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            if (e[k] == kNoContrib) break;
-            const int j = e[k] >> 1;
-            const double sg = (e[k] & 1) ? -1.0 : 1.0;  // fma by -/+1: the bits of R -/+ F*S (see tile_update)
-#pragma unroll
-            for (int q = 0; q < 5; q++) R[q] = fma(sg, (double)fs[6 * j + q], R[q]);
-        }
-        // time step in single precision (TimeStepMethod2, src/solver/TimeIntegration.cpp:8-40)
-        const float snd = gf * me.p * me.r;
-        const float lam = 0.5f * fmaf(fabsf(me.u) + snd, cg.x, fmaf(fabsf(me.v) + snd, cg.y, (fabsf(me.w) + snd) * cg.z));
-        const int c = c0 + i;
-        if (a.residual_only) {
-            const int o = a.new2old[c];
-#pragma unroll
-            for (int k = 0; k < 5; k++) a.r_out[5 * (size_t)o + k] = R[k];
-            a.dt_out[o] = (double)(a.cfl * cg.w / lam);
-        } else {
-            // W = W0 - alpha dt R / V in double (alpha dt / V = alpha cfl / lambda)
-            const double coef = a.alpha * a.cfl * rcp_nr((double)lam);
-            double W[5];
-#pragma unroll
-            for (int k = 0; k < 5; k++) W[k] = fma(-coef, R[k], W0[k]);
-            const double ir = rcp_nr(W[0]);
-            const double u = W[1] * ir, v = W[2] * ir, w = W[3] * ir;
-            const double p = (a.gamma - 1.0) * fma(-0.5, fma(W[1], u, fma(W[2], v, W[3] * w)), W[4]);
-            const double H = (W[4] + p) * ir;
-            make_rec32(a.q32out + 2 * (size_t)c, W[0], u, v, w, p, H, a.gamma);
-            if (a.last_stage) {  // the conservative state carries over exactly in double
-                const size_t sd = (size_t)a.w0_stride;
-#pragma unroll
-                for (int k = 0; k < 5; k++) a.w0[k * sd + c] = W[k];
-                a.ecell[c] = W[4] * ir;
-                r2 = R[0] * R[0];
-            }
-        }
-    }
+    if (i < nloc) r2 = tile_update_f32(a, b, c0, i, W0, cg);
     if (a.last_stage && !a.residual_only) block_sum_store(r2, partial);
 }
 

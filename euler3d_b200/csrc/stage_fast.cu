@@ -1,7 +1,7 @@
 // FP64 instantiations of the stage kernels: restructured arithmetic, fused multiply-adds where the
 // source writes fma() (built with -fmad=false, so nothing else is contracted).
 #include "common.hpp"
-#include "stage.cuh"
+#include "stage_ws.cuh"
 
 namespace e3d {
 
@@ -9,12 +9,12 @@ namespace e3d {
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes) {
     raise_smem_limit((const void *)tile_kernel<false, 4>, smem_bytes);
     raise_smem_limit((const void *)tile_kernel<false, 7>, smem_bytes);
-    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<false>, pipe_smem_bytes);
+    if (pipe_smem_bytes) raise_smem_limit((const void *)tile_ws_kernel<WS_FAST>, pipe_smem_bytes);
 }
 
 void prepare_batch_fast(size_t smem_bytes, size_t ws_smem_bytes) {
     raise_smem_limit((const void *)tile_batch_kernel<false, 6>, smem_bytes);
-    if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<false>, ws_smem_bytes);
+    if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<WS_FAST>, ws_smem_bytes);
 }
 
 // Update phase of a split stage (residual smoothing between residual and update).
@@ -29,7 +29,7 @@ void launch_batch_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaSt
 
 // The same stage with the warp-specialised persistent kernel: `grid` blocks walk the table.
 void launch_batch_ws_fast(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_ws_batch_kernel<false><<<grid, kWsThreads, smem_bytes, s>>>(bs);
+    tile_ws_batch_kernel<WS_FAST><<<grid, kWsThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;
@@ -41,8 +41,8 @@ void launch_stage_fast(const StageArgs &a, cudaStream_t s, int variant) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false, 7><<<blocks, kStageThreads, smem, s>>>(a);
     } else if (variant == 3) {
-        const size_t smem = ws_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib, a.ws_buffers);
-        tile_ws_kernel<false><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
+        const size_t smem = ws_smem_for(ws_buffer_bytes(WS_FAST, a.smem_cells, a.smem_faces, a.max_contrib), a.ws_buffers);
+        tile_ws_kernel<WS_FAST><<<a.pipe_grid, kWsThreads, smem, s>>>(a);
     } else if (variant == 2) {
         const size_t smem = tile_smem_bytes(a.smem_cells, a.smem_faces, a.max_contrib);
         tile_kernel<false, 4><<<blocks, kStageThreads, smem, s>>>(a);

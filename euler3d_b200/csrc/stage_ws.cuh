@@ -1,0 +1,271 @@
+// Warp-specialised persistent stage kernel (stage-kernel variant 3), for every precision and for
+// batches.
+//
+// One block per SM: a producer warp and kWsGroups consumer groups of kTileCells threads, over a ring
+// of B tile buffers in shared memory.  The block walks its work items blockIdx.x, + gridDim.x, ...;
+// its k-th item fills buffer k % B and is evaluated by consumer group k % kWsGroups.  The producer
+// warp streams items ahead of the consumers: for each item it waits until the item's buffer is free
+// (empty barrier), then issues every copy the tile needs onto the buffer's full barrier -- the
+// owned cell records, face records and contribution lists as bulk copies, each halo record as one
+// small bulk copy (no multicast), and L2 prefetches of the W0 rows and the cell geometry.  A consumer
+// group waits for its item's full barrier, evaluates the fluxes and the update exactly as the
+// one-block-per-tile kernels do (the same functions), with a named barrier of its own between the
+// phases, and hands the buffer back.  So copies for the next tiles are in flight while every group
+// computes, with no block launch, barrier initialisation or index chase between tiles.
+//
+// Every wait is bounded: a consumer that gives up sets the fault word of its item's solver and
+// leaves; the producer stops issuing once that fault word is set or its own wait gives up, and lets
+// every copy it issued land before it leaves.
+#pragma once
+#include "stage.cuh"
+#include "stage_f32.cuh"
+
+namespace e3d {
+
+constexpr int kWsGroups = 5;
+constexpr int kWsThreads = 32 + kWsGroups * kTileCells;
+// Bytes ahead of a batch buffer's tile data that hold the member's StageArgs.
+constexpr size_t kWsArgsSlot = (sizeof(StageArgs) + 127) & ~(size_t)127;
+static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is bulk-copied");
+
+// Precision of a warp-specialised instantiation.
+enum : int { WS_EXACT = 0, WS_FAST = 1, WS_F32 = 2 };
+
+// Bytes of one tile buffer (128-byte multiple) for the precision's layout.
+__host__ __device__ __forceinline__ size_t ws_buffer_bytes(int prec, int LC, int FC, int MC) {
+    const size_t b = prec == WS_F32 ? tile32_buf_bytes(LC, FC, MC) : tile_buf_bytes(LC, FC, MC);
+    return (b + 127) & ~(size_t)127;
+}
+
+// Dynamic shared memory with B buffers of `stride` bytes: the buffers, a full and an empty mbarrier
+// per buffer, and four doubles per consumer group for its RMS partial.
+__host__ __device__ __forceinline__ size_t ws_smem_for(size_t stride, int buffers) {
+    return (size_t)buffers * stride + 16 * (size_t)buffers + 32 * (size_t)kWsGroups;
+}
+
+// The most buffers (8 down to 2) of `stride` bytes that fit the 227 KB of a block, or 0.
+inline int ws_buffers_for(size_t stride) {
+    for (int nb = 8; nb >= 2; nb--)
+        if (ws_smem_for(stride, nb) <= 227 * 1024) return nb;
+    return 0;
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Named barrier of `threads` threads that also returns, to all of them, whether any passed true.
+__device__ __forceinline__ bool named_sync_or(int id, int threads, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(threads)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Body of the warp-specialised kernels.  Solo (BATCH false): work item k of the block is tile
+// blockIdx.x + k gridDim.x of the one solver whose arguments `solo` holds.  Batch (BATCH true): work
+// item k is entry blockIdx.x + k gridDim.x of the batch's (member, tile) table; the producer copies
+// the member's StageArgs into the buffer beside the tile's data, and the consumer group sets the
+// stage's alpha and flags in that copy before it reads it -- so each member computes what its solo
+// run computes.  A stopped member's items carry only the arguments, which the consumers skip.  A
+// wait that gives up sets the fault word of the member whose item it waited for.
+template <int PREC, bool BATCH>
+__device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage &bs, unsigned char *smem_raw) {
+    constexpr bool F32 = PREC == WS_F32, EXACT = PREC == WS_EXACT;
+    constexpr uint32_t kState = F32 ? 32u : 48u;   // bytes of a cell record
+    constexpr uint32_t kRec = F32 ? 24u : 40u;     // bytes of a face record
+    constexpr uint32_t kGeo = F32 ? 16u : 32u;     // bytes of a cell's geometry
+    const int T = kTileCells, G = gridDim.x;
+    const int B = BATCH ? bs.ws_buffers : solo.ws_buffers;
+    const int n_items = BATCH ? *bs.n_entries : solo.n_tiles;
+    const size_t slot = BATCH ? kWsArgsSlot : 0;  // the member's arguments, ahead of the tile's data
+    const size_t bb = BATCH ? (size_t)bs.ws_stride
+                            : ws_buffer_bytes(PREC, solo.smem_cells, solo.smem_faces, solo.max_contrib);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)B * bb);
+    uint64_t *empty = full + B;
+    double *gsum = reinterpret_cast<double *>(empty + B);  // [kWsGroups][4]
+    // the arguments (in global memory, or the kernel's own) of work item `item`, and its tile
+    auto item_args = [&](int item, int &tile) -> const StageArgs * {
+        if (!BATCH) {
+            tile = item;
+            return &solo;
+        }
+        const int2 e = bs.table[item];
+        tile = e.y;
+        return bs.args + 2 * e.x + bs.parity;
+    };
+    // where the tile's cell records, face records and contribution lists sit in a buffer
+    auto layout = [&](unsigned char *p, const StageArgs &a, void *&st, void *&rec, unsigned short *&ct) {
+        if (F32) {
+            const Tile32 t = tile32_at(p, a.smem_cells, a.smem_faces);
+            st = t.st, rec = t.rec, ct = t.ct;
+        } else {
+            const TileBuf t = tile_buf_at(p, a.smem_cells, a.smem_faces, a.max_contrib);
+            st = t.st, rec = t.rec, ct = t.ct;
+        }
+    };
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < B; k++) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], 1);
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 0) {  // ------------------------------------------------ producer
+        int issued = 0;  // items whose copies were issued (buffer of item k: k % B)
+        bool stopped = false;
+        for (int k = 0, item = blockIdx.x; item < n_items; k++, item += G) {
+            const int bi = k % B;
+            if (k >= B) {  // the buffer's previous item (k - B) has been handed back
+                // lane 0 waits and the warp follows its answer, so every decision is warp-uniform
+                int ok = 0;
+                if (lane == 0) {
+                    int prev_tile;
+                    int *prev_fault = item_args(item - B * G, prev_tile)->fault;
+                    const uint32_t par = (uint32_t)(((k / B) - 1) & 1);
+                    for (int it = 0; it < kWaitLimit && !ok; it++) {
+                        ok = mbar_try_wait(&empty[bi], par);
+                        if (!ok && (it & 255) == 255 && *(volatile int *)prev_fault) break;
+                    }
+                    if (!ok) atomicExch(prev_fault, 1);
+                }
+                if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                    stopped = true;
+                    break;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
+            unsigned char *base = smem_raw + (size_t)bi * bb;
+            int tile;
+            const StageArgs &a = *item_args(item, tile);
+            const bool skip = BATCH && a.ctl->done;  // a stopped member: its arguments only
+            void *st, *rec;
+            unsigned short *ct;
+            layout(base + slot, a, st, rec, ct);
+            const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
+            const int nh = skip ? 0 : a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
+            const char *qsrc = F32 ? reinterpret_cast<const char *>(a.q32in) : reinterpret_cast<const char *>(a.qin);
+            if (lane == 0) {
+                const int nf = skip ? 0 : a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+                const uint32_t b_ct = (uint32_t)a.max_contrib * T * 2u;
+                const uint32_t tile_bytes =
+                    skip ? 0u : (uint32_t)nloc * kState + round16(kRec * (uint32_t)nf) + b_ct + (uint32_t)nh * kState;
+                mbar_expect_tx(&full[bi], tile_bytes + (BATCH ? (uint32_t)sizeof(StageArgs) : 0u));
+                if (BATCH) bulk_g2s(base, &a, (uint32_t)sizeof(StageArgs), &full[bi]);
+                if (!skip) {
+                    bulk_g2s(st, qsrc + (size_t)kState * c0, (uint32_t)nloc * kState, &full[bi]);
+                    const char *rsrc = F32 ? a.tile_rec32 + a.tile_rec32_off[tile] : a.tile_rec + a.tile_rec_off[tile];
+                    bulk_g2s(rec, rsrc, round16(kRec * (uint32_t)nf), &full[bi]);
+                    bulk_g2s(ct, a.tile_contrib + (size_t)tile * a.max_contrib * T, b_ct, &full[bi]);
+                    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
+                    for (int q = 0; q < 5; q++) bulk_prefetch_l2(a.w0 + (size_t)q * a.w0_stride + c0, b_w0);
+                    const char *gsrc = F32 ? reinterpret_cast<const char *>(a.cgeo32) : reinterpret_cast<const char *>(a.cgeo);
+                    bulk_prefetch_l2(gsrc + (size_t)kGeo * c0, (uint32_t)nloc * kGeo);
+                }
+            }
+            __syncwarp();  // the expected byte count is posted before any halo copy can complete
+            if (!skip) {
+                const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+                char *hdst = static_cast<char *>(st) + (size_t)kState * nloc;
+                for (int i = lane; i < nh; i += 32)
+                    bulk_g2s(hdst + (size_t)kState * i, qsrc + (size_t)kState * hrow[i], kState, &full[bi]);
+            }
+            issued = k + 1;
+        }
+        // every copy issued must land before the block can leave (the consumers wait for them when
+        // the walk completes; after a give-up they may not have)
+        if (lane == 0 && stopped) {
+            for (int k = (issued > B ? issued - B : 0); k < issued; k++)
+                tile_drain(&full[k % B], (uint32_t)((k / B) & 1));
+        }
+        return;
+    }
+
+    // ------------------------------------------------------------------ consumer group
+    const int grp = (threadIdx.x - 32) / T;
+    const int tid = (threadIdx.x - 32) % T;
+    const int bar_id = 1 + grp;
+    double *fsum = gsum + 4 * grp;
+    for (int k = grp, item = blockIdx.x + grp * G; item < n_items; k += kWsGroups, item += kWsGroups * G) {
+        const int bi = k % B;
+        unsigned char *base = smem_raw + (size_t)bi * bb;
+        int tile;
+        const StageArgs *ag = item_args(item, tile);  // global (batch) or the kernel's own arguments
+        bool ok = false;
+        const int polls = ag->wait_polls;
+        for (int it = 0; it < polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)((k / B) & 1));
+        if (!ok) atomicExch(ag->fault, 1);
+        if (BATCH && ok && tid == 0) {  // this stage's alpha and flags in the member's arguments
+            StageArgs *sa = reinterpret_cast<StageArgs *>(base);
+            sa->alpha = bs.alpha;
+            sa->first_stage = bs.first_stage;
+            sa->last_stage = bs.last_stage;
+            sa->residual_only = 0;
+        }
+        if (named_sync_or(bar_id, T, !ok)) return;  // the same decision for the whole group
+        const StageArgs &a = BATCH ? *reinterpret_cast<const StageArgs *>(base) : solo;
+        const bool run = !BATCH || !a.ctl->done;  // the member of a batch item may have stopped
+        double r2 = 0.0;
+        if (run) {
+            const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
+            const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+            if (F32) {
+                const Tile32 b = tile32_at(base + slot, a.smem_cells, a.smem_faces);
+                tile_fluxes_f32(a, b, nf, c0, tid, T);
+                double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                float4 cg = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (tid < nloc) tile_load_cell_f32(a, c0 + tid, W0, cg);
+                named_sync(bar_id, T);
+                if (tid < nloc) r2 = tile_update_f32(a, b, c0, tid, W0, cg);
+            } else {
+                const TileBuf b = tile_buf_at(base + slot, a.smem_cells, a.smem_faces, a.max_contrib);
+                double *fs = reinterpret_cast<double *>(b.rec);
+                tile_fluxes<EXACT, kTileCells>(a, b, fs, nf, c0, tid);
+                double W0[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                double4 cg = make_double4(0.0, 0.0, 0.0, 0.0);
+                if (tid < nloc) tile_load_cell(a, c0, tid, W0, cg);
+                named_sync(bar_id, T);
+                if (tid < nloc) r2 = tile_update<EXACT>(a, b, fs, c0, tid, W0, cg);
+            }
+        }
+        const bool sum = run && a.last_stage && !a.residual_only;  // uniform across the group
+        double *partial = sum ? a.partials + tile : nullptr;
+        if (sum) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+            if ((tid & 31) == 0) fsum[tid >> 5] = r2;
+        }
+        named_sync(bar_id, T);  // every read of the buffer (the arguments included) is done
+        if (tid == 0) {
+            // the order of block_sum_store's last shuffle tree, so every kernel writes the same partial
+            if (sum) *partial = (fsum[0] + fsum[2]) + (fsum[1] + fsum[3]);
+            mbar_arrive(&empty[bi]);
+        }
+        if (sum) named_sync(bar_id, T);  // fsum is reused by the next item
+    }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_kernel(StageArgs a) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ws_body<PREC, false>(a, BatchStage{}, smem_raw);
+}
+
+// Several solvers in one persistent grid: the batch's (member, tile) table walked as above.
+template <int PREC>
+__global__ void __launch_bounds__(kWsThreads, 1) tile_ws_batch_kernel(BatchStage bs) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ws_body<PREC, true>(StageArgs{}, bs, smem_raw);
+}
+
+}  // namespace e3d

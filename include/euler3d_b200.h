@@ -212,10 +212,10 @@ typedef struct e3d_run_params {
 	                                     so the stages are timed as they run back to back
 	                                     (stats.stage_ms over the iterations that ran) */
 	int32_t stage_kernel;             /* 0: the autotuned stage kernel; 1, 2: per-cell gather with two
-	                                     register budgets; 3: face tiles; 4: persistent face tiles with
-	                                     a producer warp streaming tiles to consumer warps (FP64 modes;
-	                                     in FP32_FLUX: face tiles at eight blocks per SM); 5: face tiles
-	                                     at seven blocks per SM (FP64 only) (kept for later runs) */
+	                                     register budgets (FP64 modes); 3: face tiles; 4: persistent
+	                                     face tiles with a producer warp streaming tiles to consumer
+	                                     warps; 5: face tiles at seven blocks per SM (FP64) or eight
+	                                     (FP32_FLUX) (kept for later runs) */
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
 	                                     No counterpart in the reference, whose test is absolute. */
@@ -351,8 +351,7 @@ e3d_status e3d_batch_retire(e3d_batch *batch, e3d_solver **solvers, e3d_run_stat
 /* Takes `solver` out of the batch whether or not its run has stopped; stats as e3d_batch_retire. */
 e3d_status e3d_batch_remove(e3d_batch *batch, e3d_solver *solver, e3d_run_stats *stats);
 
-/* The stage kernel of a batch's launches (FP64 and FP64_EXACT batches; an FP32_FLUX batch always
- * runs the first):
+/* The stage kernel of a batch's launches:
  *   E3D_BATCH_KERNEL_TILES  one block of 128 threads per (member, tile) entry of the table (default)
  *   E3D_BATCH_KERNEL_WS     one persistent block per SM walking the table: a producer warp copies each
  *                           entry's member arguments and tile data into a ring of shared-memory buffers

@@ -61,7 +61,7 @@ def collect(solver, stats):
 
 
 @pytest.mark.parametrize("precision,kernel", [(p, _lib.BATCH_KERNEL_TILES) for p in PRECISIONS] +
-                         [(_lib.PREC_FP64_EXACT, _lib.BATCH_KERNEL_WS), (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+                         [(p, _lib.BATCH_KERNEL_WS) for p in PRECISIONS])
 def test_mix_equals_alone(precision, kernel):
     refs = [alone(n, sc, sd, precision, rp) for n, sc, sd, rp in MIX]
     b = Batch()
@@ -85,7 +85,8 @@ def test_mix_equals_alone(precision, kernel):
 
 @pytest.mark.parametrize("precision,kernel", [(_lib.PREC_FP64, _lib.BATCH_KERNEL_TILES),
                                               (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_TILES),
-                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS),
+                                              (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_WS)])
 def test_staggered_admission(precision, kernel):
     """Members join a running batch between steps (continuous admission) and leave as they stop."""
     refs = [alone(n, sc, sd, precision, rp) for n, sc, sd, rp in MIX]

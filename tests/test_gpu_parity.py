@@ -315,6 +315,25 @@ def test_fp32_deterministic():
     assert np.array_equal(runs[0][1], runs[1][1])
 
 
+def test_fp32_kernels_agree():
+    """Every FP32_FLUX stage kernel (face tiles at two register budgets, the warp-specialised
+    persistent kernel) computes the same bits: the arithmetic is fixed by the source."""
+    name = "ogrid"
+    flow = CASES[name].flow(precision=_lib.PREC_FP32_FLUX, ordering=_lib.ORDER_SPATIAL)
+    arrays = prepared(name)
+    st = perturbed_state(arrays, flow, seed=17)
+    runs = []
+    for kernel in (_lib.KERNEL_TILE, _lib.KERNEL_TILE_PIPE, _lib.KERNEL_TILE_B3):
+        s = EulerSolver(arrays, flow)
+        s.set_state(st)
+        s.run(25, stage_kernel=kernel)
+        runs.append((s.get_state(), s.rms_history()))
+    for g, h in runs[1:]:
+        for k in STATE_KEYS:
+            assert np.array_equal(g[k], runs[0][0][k]), k
+        assert np.array_equal(h, runs[0][1])
+
+
 def test_fp32_converged_fields_and_forces():
     """FP32_FLUX mode against the double oracle converged to a 1e-8 density-residual drop.
 

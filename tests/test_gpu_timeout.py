@@ -23,13 +23,14 @@ from euler3d_b200.solver import EulerSolver
 
 pytestmark = pytest.mark.gpu
 
-# (precision, stage kernel) pairs with bounded waits: face tiles, pipelined face tiles, the
-# seven-blocks-per-SM face tiles (FP64 only) and the FP32_FLUX face tiles
+# (precision, stage kernel) pairs with bounded waits: face tiles, the warp-specialised persistent
+# kernel and face tiles at seven (FP64) or eight (FP32_FLUX) blocks per SM
 WAITING_KERNELS = [
     (_lib.PREC_FP64_EXACT, _lib.KERNEL_TILE),
     (_lib.PREC_FP64_EXACT, _lib.KERNEL_TILE_PIPE),
     (_lib.PREC_FP64, _lib.KERNEL_TILE_B3),
-    (_lib.PREC_FP32_FLUX, _lib.KERNEL_TILE_PIPE),  # FP32_FLUX variant 3: face tiles at eight blocks/SM
+    (_lib.PREC_FP32_FLUX, _lib.KERNEL_TILE_PIPE),
+    (_lib.PREC_FP32_FLUX, _lib.KERNEL_TILE_B3),
 ]
 
 
@@ -82,7 +83,8 @@ def test_timeout_stops_run_and_solver_recovers(precision, kernel):
 
 @pytest.mark.parametrize("precision,kernel", [(_lib.PREC_FP64, _lib.BATCH_KERNEL_TILES),
                                               (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_TILES),
-                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS)])
+                                              (_lib.PREC_FP64, _lib.BATCH_KERNEL_WS),
+                                              (_lib.PREC_FP32_FLUX, _lib.BATCH_KERNEL_WS)])
 def test_timeout_in_batch_member(precision, kernel):
     """A member whose waits give up is retired with E3D_ERR_TIMEOUT; the member beside it is not
     disturbed (it equals its run alone bit for bit), and the timed-out solver runs normally once
