@@ -1,13 +1,16 @@
 // Warp-specialised persistent stage kernel (stage-kernel variant 3), for every precision and for
 // batches.
 //
-// One block per SM: a producer warp and kWsGroups consumer groups of kTileCells threads, over a ring
-// of B tile buffers in shared memory.  The block walks its work items blockIdx.x, + gridDim.x, ...;
-// its k-th item fills buffer k % B and is evaluated by consumer group k % kWsGroups.  The producer
-// warp streams items ahead of the consumers: for each item it waits until the item's buffer is free
-// (empty barrier), then issues every copy the tile needs onto the buffer's full barrier -- the
-// owned cell records, face records and contribution lists as bulk copies, each halo record as one
-// small bulk copy (no multicast), and L2 prefetches of the W0 rows and the cell geometry.  A consumer
+// One block per SM: a producer warp and up to kWsGroups consumer groups of kTileCells threads, each
+// group with a ring of D tile buffers of its own in shared memory.  The block walks its work items
+// blockIdx.x, + gridDim.x, ...; its k-th item goes to group g = k % Gc, whose j-th item (j = k / Gc)
+// fills the group's buffer j % D.  A buffer has one consumer, which takes its fills in order, so a
+// parity wait on its barriers always refers to the next phase.  The producer warp streams items
+// ahead of the consumers: for each item it waits until the item's buffer is free (empty barrier),
+// then issues every copy the tile needs onto the buffer's full barrier -- the owned cell records,
+// face records and contribution lists as bulk copies (no multicast), the halo records as 16-byte
+// cp.async by the 32 lanes, each lane's completion arriving on the barrier
+// (cp.async.mbarrier.arrive.noinc), and L2 prefetches of the W0 rows and the cell geometry.  A consumer
 // group waits for its item's full barrier, evaluates the fluxes and the update exactly as the
 // one-block-per-tile kernels do (the same functions), with a named barrier of its own between the
 // phases, and hands the buffer back.  So copies for the next tiles are in flight while every group
@@ -43,11 +46,31 @@ __host__ __device__ __forceinline__ size_t ws_smem_for(size_t stride, int buffer
     return (size_t)buffers * stride + 16 * (size_t)buffers + 32 * (size_t)kWsGroups;
 }
 
-// The most buffers (8 down to 2) of `stride` bytes that fit the 227 KB of a block, or 0.
+// Consumer groups for B buffers: one buffer per group up to kWsGroups groups, then more per group.
+__host__ __device__ __forceinline__ int ws_groups_for(int buffers) {
+    return buffers < kWsGroups ? buffers : kWsGroups;
+}
+
+// Buffers of `stride` bytes for the block: as many as fit its 227 KB (at most two per group), made a
+// multiple of the group count; 0 when not even three fit.
 inline int ws_buffers_for(size_t stride) {
-    for (int nb = 8; nb >= 2; nb--)
-        if (ws_smem_for(stride, nb) <= 227 * 1024) return nb;
-    return 0;
+    int fit = 0;
+    for (int nb = 2 * kWsGroups; nb >= 1 && !fit; nb--)
+        if (ws_smem_for(stride, nb) <= 227 * 1024) fit = nb;
+    if (fit < 3) return 0;
+    const int g = ws_groups_for(fit);
+    return g * (fit / g);
+}
+
+// Halo records of an item: 16-byte cp.async by the producer's lanes.
+__device__ __forceinline__ void ws_halo_gather(char *dst, const char *src, uint32_t bytes) {
+    for (uint32_t o = 0; o < bytes; o += 16) cp_async16(dst + o, src + o);
+}
+
+// This lane's cp.async operations issued so far arrive on bar when they complete (one arrival,
+// counted in the barrier's expected arrivals).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void named_sync(int id, int threads) {
@@ -84,6 +107,13 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     constexpr uint32_t kGeo = F32 ? 16u : 32u;     // bytes of a cell's geometry
     const int T = kTileCells, G = gridDim.x;
     const int B = BATCH ? bs.ws_buffers : solo.ws_buffers;
+    const int Gc = ws_groups_for(B), D = B / Gc;  // consumer groups, buffers per group
+    // buffer and fill number of the block's k-th item
+    auto buffer_of = [&](int k, int &fill) {
+        const int j = k / Gc;
+        fill = j / D;
+        return (k % Gc) * D + j % D;
+    };
     const int n_items = BATCH ? *bs.n_entries : solo.n_tiles;
     const size_t slot = BATCH ? kWsArgsSlot : 0;  // the member's arguments, ahead of the tile's data
     const size_t bb = BATCH ? (size_t)bs.ws_stride
@@ -113,7 +143,7 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     };
     if (threadIdx.x == 0) {
         for (int k = 0; k < B; k++) {
-            mbar_init(&full[k], 1);
+            mbar_init(&full[k], 1 + 32);  // the producer's expect-tx arrival + one per lane's cp.async
             mbar_init(&empty[k], 1);
         }
     }
@@ -121,17 +151,18 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 0) {  // ------------------------------------------------ producer
-        int issued = 0;  // items whose copies were issued (buffer of item k: k % B)
+        int issued = 0;  // items whose copies were issued
         bool stopped = false;
         for (int k = 0, item = blockIdx.x; item < n_items; k++, item += G) {
-            const int bi = k % B;
-            if (k >= B) {  // the buffer's previous item (k - B) has been handed back
+            int fill;
+            const int bi = buffer_of(k, fill);
+            if (fill >= 1) {  // the buffer's previous item (k - B) has been handed back
                 // lane 0 waits and the warp follows its answer, so every decision is warp-uniform
                 int ok = 0;
                 if (lane == 0) {
                     int prev_tile;
                     int *prev_fault = item_args(item - B * G, prev_tile)->fault;
-                    const uint32_t par = (uint32_t)(((k / B) - 1) & 1);
+                    const uint32_t par = (uint32_t)((fill - 1) & 1);
                     for (int it = 0; it < kWaitLimit && !ok; it++) {
                         ok = mbar_try_wait(&empty[bi], par);
                         if (!ok && (it & 255) == 255 && *(volatile int *)prev_fault) break;
@@ -157,8 +188,7 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
             if (lane == 0) {
                 const int nf = skip ? 0 : a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
                 const uint32_t b_ct = (uint32_t)a.max_contrib * T * 2u;
-                const uint32_t tile_bytes =
-                    skip ? 0u : (uint32_t)nloc * kState + round16(kRec * (uint32_t)nf) + b_ct + (uint32_t)nh * kState;
+                const uint32_t tile_bytes = skip ? 0u : (uint32_t)nloc * kState + round16(kRec * (uint32_t)nf) + b_ct;
                 mbar_expect_tx(&full[bi], tile_bytes + (BATCH ? (uint32_t)sizeof(StageArgs) : 0u));
                 if (BATCH) bulk_g2s(base, &a, (uint32_t)sizeof(StageArgs), &full[bi]);
                 if (!skip) {
@@ -172,20 +202,24 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
                     bulk_prefetch_l2(gsrc + (size_t)kGeo * c0, (uint32_t)nloc * kGeo);
                 }
             }
-            __syncwarp();  // the expected byte count is posted before any halo copy can complete
             if (!skip) {
                 const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
                 char *hdst = static_cast<char *>(st) + (size_t)kState * nloc;
                 for (int i = lane; i < nh; i += 32)
-                    bulk_g2s(hdst + (size_t)kState * i, qsrc + (size_t)kState * hrow[i], kState, &full[bi]);
+                    ws_halo_gather(hdst + (size_t)kState * i, qsrc + (size_t)kState * hrow[i], kState);
             }
+            cp_async_arrive_noinc(&full[bi]);  // every lane, with or without halo copies
             issued = k + 1;
         }
         // every copy issued must land before the block can leave (the consumers wait for them when
         // the walk completes; after a give-up they may not have)
+        asm volatile("cp.async.wait_all;" ::: "memory");
         if (lane == 0 && stopped) {
-            for (int k = (issued > B ? issued - B : 0); k < issued; k++)
-                tile_drain(&full[k % B], (uint32_t)((k / B) & 1));
+            for (int k = (issued > B ? issued - B : 0); k < issued; k++) {
+                int fill;
+                const int bi = buffer_of(k, fill);
+                tile_drain(&full[bi], (uint32_t)(fill & 1));
+            }
         }
         return;
     }
@@ -193,16 +227,18 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     // ------------------------------------------------------------------ consumer group
     const int grp = (threadIdx.x - 32) / T;
     const int tid = (threadIdx.x - 32) % T;
+    if (grp >= Gc) return;  // fewer groups than the block has (large tiles: fewer buffers)
     const int bar_id = 1 + grp;
     double *fsum = gsum + 4 * grp;
-    for (int k = grp, item = blockIdx.x + grp * G; item < n_items; k += kWsGroups, item += kWsGroups * G) {
-        const int bi = k % B;
+    for (int k = grp, item = blockIdx.x + grp * G; item < n_items; k += Gc, item += Gc * G) {
+        int fill;
+        const int bi = buffer_of(k, fill);
         unsigned char *base = smem_raw + (size_t)bi * bb;
         int tile;
         const StageArgs *ag = item_args(item, tile);  // global (batch) or the kernel's own arguments
         bool ok = false;
         const int polls = ag->wait_polls;
-        for (int it = 0; it < polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)((k / B) & 1));
+        for (int it = 0; it < polls && !ok; it++) ok = mbar_try_wait(&full[bi], (uint32_t)(fill & 1));
         if (!ok) atomicExch(ag->fault, 1);
         if (BATCH && ok && tid == 0) {  // this stage's alpha and flags in the member's arguments
             StageArgs *sa = reinterpret_cast<StageArgs *>(base);
