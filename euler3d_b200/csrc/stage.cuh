@@ -17,6 +17,7 @@
 //   ghost[8G]         ghost cells, 8 doubles each: rho u v w p E H M
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "euler3d_b200.h"
@@ -941,20 +942,26 @@ struct BatchStage {
     int first_stage, last_stage, parity;
     int ws_buffers, ws_stride;           // tile_ws_batch_kernel: buffers, bytes per buffer
 };
-static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is copied in 8-byte words");
+static_assert(sizeof(StageArgs) % 4 == 0, "StageArgs is copied in 4-byte words");
 
-// The block's member arguments into shared memory, with the stage's own alpha and flags.
+// The block's member arguments into shared memory, with the stage's own alpha and flags written in
+// place of the member's as the words are copied (one barrier).
 __device__ __forceinline__ int2 batch_stage_args(const BatchStage &bs, StageArgs *sa) {
     const int2 e = bs.table[blockIdx.x];
-    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(bs.args + 2 * e.x + bs.parity);
-    unsigned long long *dst = reinterpret_cast<unsigned long long *>(sa);
-    for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / 8); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        sa->alpha = bs.alpha;
-        sa->first_stage = bs.first_stage;
-        sa->last_stage = bs.last_stage;
-        sa->residual_only = 0;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(bs.args + 2 * e.x + bs.parity);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(sa);
+    constexpr int kAlpha = (int)(offsetof(StageArgs, alpha) / 4), kFirst = (int)(offsetof(StageArgs, first_stage) / 4);
+    constexpr int kLast = (int)(offsetof(StageArgs, last_stage) / 4);
+    constexpr int kResidual = (int)(offsetof(StageArgs, residual_only) / 4);
+    const unsigned long long alpha = (unsigned long long)__double_as_longlong(bs.alpha);
+    for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / 4); i += blockDim.x) {
+        uint32_t v = src[i];
+        if (i == kAlpha) v = (uint32_t)alpha;
+        else if (i == kAlpha + 1) v = (uint32_t)(alpha >> 32);
+        else if (i == kFirst) v = (uint32_t)bs.first_stage;
+        else if (i == kLast) v = (uint32_t)bs.last_stage;
+        else if (i == kResidual) v = 0u;
+        dst[i] = v;
     }
     __syncthreads();
     return e;
