@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--batch-kernel", choices=["tiles", "ws"], default="tiles",
                     help="kernels mode: the batch stage kernel (one block per tile, or warp-specialised)")
     ap.add_argument("--iters", type=int, default=2, help="profile mode: RK5 iterations")
+    ap.add_argument("--ref-mesh", choices=["c3", "c1"], default="c3",
+                    help="reference arm: the bench mesh (c3) or the 64x32x2 bump channel of config 1 (Mach 0.5, CFL 1.5)")
+    ap.add_argument("--ref-ranks", type=int, default=0, help="reference arm: MPI ranks (0: one per host core)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the first iteration against the CPU oracle")
     ap.add_argument("--served-requests", type=int, default=48)
@@ -504,13 +507,18 @@ def run_reference(args, rank, world):
 
     K, W = args.steps, max(args.warmup, 3)
     cores = host_cores()
-    raw = meshgen.bump_box_tets(args.n)
+    if args.ref_mesh == "c1":
+        raw, mach, cfl = meshgen.bump_channel(64, 32, 2), 0.5, 1.5
+        workload = "bump_channel 64x32x2 (4,096 hexahedra), Mach 0.5, Roe, RK5, CFL 1.5"
+    else:
+        raw, mach, cfl = meshgen.bump_box_tets(args.n), 0.6, 1.0
+        workload = WORKLOAD
     cells = raw.n_cells
     if os.path.exists(REF_MPI):
-        ranks = max(1, min(cores, 64))
+        ranks = args.ref_ranks if args.ref_ranks > 0 else max(1, min(cores, 64))
         arrays = Mesh.from_raw(raw).arrays()
         with tempfile.TemporaryDirectory(prefix="e3dref") as d:
-            res = run_reference_mpi(raw, arrays, ranks, W, K, 0.6, 1.0, d)
+            res = run_reference_mpi(raw, arrays, ranks, W, K, mach, cfl, d)
         assert res["cells"] == cells and res["iterations"] == K, res
         tmax = res["seconds"]
         value = 5.0 * cells * K / tmax
@@ -520,15 +528,15 @@ def run_reference(args, rank, world):
                   f"x-slab partitions, the reference's halo exchange over a shared-memory MPI), {K} timed RK5 "
                   f"iterations after {W} untimed; slowest rank {tmax:.2f} s; mesh connectivity set up by the "
                   f"library's numbering-identical preparation ({res['setup_seconds']:.1f} s setup)")
-        config = {"workload": WORKLOAD, "cells": cells, "ranks": ranks, "build": "-Ofast (reference Release)",
-                  "same_mesh": True}
+        config = {"workload": workload, "cells": cells, "ranks": ranks, "host_cores": cores,
+                  "build": "-Ofast (reference Release)", "same_mesh": args.ref_mesh == "c3"}
     else:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle as po  # the CPU baseline only
 
         arrays = Mesh.from_raw(raw).arrays()
         m = po.Mesh(arrays)
-        fl = po.flow(0.6, 0.0, 1.4, 1.0)
+        fl = po.flow(mach, 0.0, 1.4, cfl)
         s = po.freestream(m, fl)
         po.run(m, fl, s, 1)
         t = time.time()
@@ -539,7 +547,7 @@ def run_reference(args, rank, world):
         kind = "port"
         sample = (f"CPU oracle port (the reference binary is not built), 1 RK5 iteration of the full {cells}-cell "
                   f"mesh, 1 thread, scaled to {K} steps")
-        config = {"workload": WORKLOAD, "cells": cells, "ranks": 1, "same_mesh": True}
+        config = {"workload": workload, "cells": cells, "ranks": 1, "same_mesh": args.ref_mesh == "c3"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": tmax * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
