@@ -92,6 +92,42 @@ def served_leg(args) -> dict:
     return out
 
 
+def batch_leg(device: int, peak: float) -> dict:
+    """Batched members (configuration 4's shape): 64 bump channels of about 20k and of about 80k
+    cells (Mach 0.30-0.615, CFL 1.5, Roe) advanced together, FP64 and FP32_FLUX, 20 RK5 iterations
+    timed after 4 untimed; cell-stage updates per second over the members, and the stage kernel's
+    roofline fraction from the algorithmic bytes of the members' meshes (the graph's device time
+    includes the per-iteration RMS / coefficient kernels, so the fraction is a lower bound)."""
+    from euler3d_b200 import _lib, meshgen
+    from euler3d_b200.batch import Batch
+    from euler3d_b200.solver import EulerSolver, FlowConfig, Mesh
+
+    out = {}
+    for nx, ny in ((140, 70), (280, 140)):
+        arrays = Mesh.from_raw(meshgen.bump_channel(nx, ny, 2)).arrays()
+        n, f = int(arrays["n_cells"]), int(arrays["n_faces"])
+        for prec, name in ((_lib.PREC_FP64, "fp64"), (_lib.PREC_FP32_FLUX, "fp32")):
+            members = [EulerSolver(arrays, FlowConfig(mach=0.3 + 0.005 * i, cfl=1.5, precision=prec,
+                                                      ordering=_lib.ORDER_SPATIAL, device=device), autotune=False)
+                       for i in range(64)]
+            b = Batch(device)
+            for m in members:
+                b.add(m, 100)
+            b.step(4)
+            b.step(20)
+            ms = b.info()["last_step_ms"]
+            b.close()
+            for m in members:
+                m.close()
+            rate = 5.0 * 20 * 64 * n / (ms / 1e3)
+            bpc = algorithmic_bytes_per_cell_stage(n, f, fp32=prec == _lib.PREC_FP32_FLUX)
+            out[f"{n}_cells_{name}"] = {"members": 64, "cells_per_member": n, "faces_per_cell": f / n,
+                                        "step_ms_20_iterations": ms, "cell_stage_updates_per_s": rate,
+                                        "bytes_per_cell_stage": bpc, "achieved_GBs": rate * bpc / 1e9,
+                                        "frac_of_measured_peak": rate * bpc / 1e9 / peak}
+    return out
+
+
 def algorithmic_bytes_per_cell_stage(n_cells: int, n_faces: int, fp32: bool = False) -> float:
     """Bytes per cell-stage, each array counted once with ideal gather reuse (f_c = faces per cell).
     FP64: 160 + 40 f_c -- read W, read U0, write W (3 x 40 B), 1/5 of writing U0 (8 B), volume
@@ -360,6 +396,8 @@ def run_ours(args, rank, world, local_rank):
     }
     solver.close()
     del arrays
+    if rank == 0 and world == 1 and args.mode == "all":
+        line["batch"] = batch_leg(local_rank, peak)
     if rank == 0 and world == 1 and args.mode == "all" and args.served_requests > 0:
         line["served"] = served_leg(args)
     if rank == 0:
