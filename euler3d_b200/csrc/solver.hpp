@@ -408,6 +408,7 @@ struct Solver {
         double *r0 = rbuf.p, *r1 = rbuf.p + n5, *r2 = rbuf.p + 2 * n5;
         StageArgs ar = a;
         ar.split = 1;
+        ar.ghost_out = a.last_stage;  // the residual phase of the last stage leaves the ghosts
         ar.last_stage = 0;
         ar.r_dev = r0;
         launch_stage(ar);

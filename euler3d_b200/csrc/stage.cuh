@@ -118,6 +118,8 @@ struct StageArgs {
                                      // summed sequentially like EulerSolver::computeRMS; else null
     int wait_polls;                  // polls of a tile's data barrier before the wait gives up (kWaitLimit;
                                      // fewer, down to 0, only to exercise the timeout path)
+    int ghost_out;                   // write wall / symmetry ghost records although this is not a last
+                                     // stage (the residual phase of a split last stage)
 };
 
 // One face of a tile: code = l | r << 10 | tag << 20 (local cell indices; r unused for boundary
@@ -374,15 +376,29 @@ __device__ __forceinline__ void ghost_finish(double *gp, double g, double rho, d
     out = Prim{rho, u, v, w, p, H};
 }
 
-// BC::Wall / BC::Symmetry (src/solver/PhysicalBC.cpp:124-231): mirrored velocity.
+// BC::Wall / BC::Symmetry (src/solver/PhysicalBC.cpp:124-231): mirrored velocity.  The kernels
+// never read a wall or symmetry ghost back (it is rebuilt from its interior cell at every stage), so
+// its record is written only when `store` says so (the last stage of an iteration, and
+// e3d_solver_residual): the state a run leaves is the same, with a fifth of the ghost writes.
+// Without the store only what the face flux needs is formed (H for symmetry faces).
 __device__ __forceinline__ void ghost_mirror(double *gp, double g, const Prim &d, double nx, double ny, double nz,
-                                             Prim &out) {
-    double c = sqrt(g * (d.p / d.rho));
+                                             Prim &out, bool store, bool need_h) {
     double V = d.u * nx + d.v * ny + d.w * nz;
     double u = d.u - 2 * V * nx;
     double v = d.v - 2 * V * ny;
     double w = d.w - 2 * V * nz;
-    ghost_finish(gp, g, d.rho, u, v, w, d.p, c, out);
+    if (store) {
+        double c = sqrt(g * (d.p / d.rho));
+        ghost_finish(gp, g, d.rho, u, v, w, d.p, c, out);
+    } else {
+        double H = 0.0;
+        if (need_h) {  // ghost_finish's E and H, in its operation order
+            double q2 = u * u + v * v + w * w;
+            double E = d.p / ((g - 1) * d.rho) + (q2 / 2.0);
+            H = E + (d.p / d.rho);
+        }
+        out = Prim{d.rho, u, v, w, d.p, H};
+    }
 }
 
 // Farfield ghost (EulerSolver::updateBC, src/solver/EulerSolver.cpp:205-227): the branch comes
@@ -456,8 +472,9 @@ __device__ __forceinline__ void block_sum_store(double v, double *dst) {
 __device__ __forceinline__ bool boundary_face(const StageArgs &a, int tag, double *gp, int c, const Prim &me,
                                               const double4 &fg, double F[5], Prim &gs) {
     const double g = a.gamma;
+    const bool store = a.last_stage || a.residual_only || a.ghost_out;
     if (tag == TAG_WALL) {
-        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs, store, false);
         F[0] = 0;
         F[1] = fg.x * gs.p;
         F[2] = fg.y * gs.p;
@@ -466,7 +483,7 @@ __device__ __forceinline__ bool boundary_face(const StageArgs &a, int tag, doubl
         return false;
     }
     if (tag == TAG_SYM) {
-        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs);
+        ghost_mirror(gp, g, me, fg.x, fg.y, fg.z, gs, store, true);
         return true;
     }
     if (tag == TAG_FAR) {
