@@ -33,7 +33,7 @@ from .solver import EulerSolver, FlowConfig, Mesh
 class SolveRequest:
     rid: int
     arrival: float            # seconds after the stream starts
-    family: str               # "channel" (bump channel, hexahedra) or "ogrid" (biconvex O-grid, prisms; channel above 1M cells)
+    family: str               # "channel" (bump channel, hexahedra) or "ogrid" (biconvex O-grid, prisms; channel above 600k cells)
     cells: int                # requested size; the generated mesh has about this many cells
     mach: float
     aoa: float                # degrees
@@ -92,9 +92,10 @@ def request_mesh(req: SolveRequest) -> mg.RawMesh:
     at 1.1, and its span layers are 0.1 chord thick, thinner on grids finer than 128 radial layers:
     the reference's tetrahedron volume (from edge lengths, src/mesh/Metrics.cpp:311-331) loses a
     flat cell's volume to cancellation when its span edges are long against its in-plane ones,
-    which happens first at the sharp leading and trailing edges of a fine grid.  Above 1M cells
-    the O-grid's slivers still lose their volume that way, so those requests get a channel."""
-    if req.family == "ogrid" and req.cells <= 1_000_000:
+    which happens first at the sharp leading and trailing edges of a fine grid.  Above about 800k
+    cells the O-grid's slivers still lose their volume that way (measured: the smallest such grid
+    of a sweep over 200k-1M cells had 815,863 cells), so requests above 600k cells get a channel."""
+    if req.family == "ogrid" and req.cells <= 600_000:
         nj = max(4, int(round(math.sqrt(req.cells / 8.0))))
         dz = 0.1 * min(1.0, 128.0 / nj)
         return mg.biconvex_ogrid(2 * nj, nj, 2, seed=req.seed % 1000, stretch=1.1 ** (128.0 / nj), span=2 * dz)
@@ -161,6 +162,7 @@ def summarize(results: Sequence[SolveResult], t_end: Optional[float] = None) -> 
                              "p99_latency_s": percentile([r.latency for r in rs], 99),
                              "converged_p50_latency_s": percentile([r.latency for r in ok], 50)}
     return {"solves": len(results), "seconds": t1 - t0, "solves_per_s": len(results) / span, "by_drop": by_drop,
+            "refused": sum(r.status not in (_lib.E3D_OK, _lib.E3D_ERR_NONFINITE, _lib.E3D_ERR_TIMEOUT) for r in results),
             "converged": converged, "converged_solves_per_s": converged / span,
             "capped": sum(r.status == _lib.E3D_OK and r.stop_reason == _lib.STOP_MAX_ITER for r in results),
             "diverged": sum(r.status == _lib.E3D_ERR_NONFINITE for r in results),
@@ -241,7 +243,13 @@ class Server:
                     preparing.append((req, fut))
                 while preparing and preparing[0][1].done():
                     req, fut = preparing.popleft()
-                    arrays = fut.result()
+                    try:
+                        arrays = fut.result()
+                    except _lib.E3DError as e:  # a mesh the preparation refuses: a failed request
+                        results.append(SolveResult(req.rid, req.cells, req.arrival, math.nan, self.clock() - t0, 0,
+                                                   -1, e.status, math.nan, math.nan, math.nan, math.nan, 0,
+                                                   drop=req.drop))
+                        continue
                     est = footprint_estimate(int(arrays["n_cells"]), int(arrays["n_faces"]), first)
                     ready.append((req, arrays, est))
                 # admission by device-memory footprint, first come first served
@@ -349,7 +357,13 @@ def serve_plain(requests: Sequence[SolveRequest], device: int = 0, precision: in
             t.start()
             timers.append(t)
         for req, f in zip(reqs, futures):
-            arrays = f.result()
+            try:
+                arrays = f.result()
+            except _lib.E3DError as e:  # a mesh the preparation refuses: a failed request
+                now = clock() - t0
+                results.append(SolveResult(req.rid, req.cells, req.arrival, now, now, 0, -1, e.status, math.nan,
+                                           math.nan, math.nan, math.nan, 0, drop=req.drop))
+                continue
             started = clock() - t0
             s = EulerSolver(arrays, request_flow(req, precision))
             status = _lib.E3D_OK
