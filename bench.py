@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--batch-kernel", choices=["tiles", "ws"], default="tiles",
                     help="kernels mode: the batch stage kernel (one block per tile, or warp-specialised)")
     ap.add_argument("--iters", type=int, default=2, help="profile mode: RK5 iterations")
+    ap.add_argument("--channel", type=int, nargs=2, default=None, metavar=("NX", "NY"),
+                    help="profile mode: a 2-layer bump channel of NX x NY x 2 hexahedra instead of the tetrahedral box")
     ap.add_argument("--ref-mesh", choices=["c3", "c1"], default="c3",
                     help="reference arm: the bench mesh (c3) or the 64x32x2 bump channel of config 1 (Mach 0.5, CFL 1.5)")
     ap.add_argument("--ref-ranks", type=int, default=0, help="reference arm: MPI ranks (0: one per host core)")
@@ -452,9 +454,13 @@ def profile_case(args, device):
 
     prec = {"fp64": _lib.PREC_FP64, "fp64_exact": _lib.PREC_FP64_EXACT, "fp32": _lib.PREC_FP32_FLUX}[args.precision]
     order = {"spatial": _lib.ORDER_SPATIAL, "rcm": _lib.ORDER_RCM, "native": _lib.ORDER_NATIVE}[args.ordering]
-    arrays = Mesh.from_raw(meshgen.bump_box_tets(args.n)).arrays()
-    s = EulerSolver(arrays, FlowConfig(mach=0.6, cfl=1.0, precision=prec, ordering=order, device=device),
-                    autotune=args.kernel == 0)
+    if args.channel:
+        arrays = Mesh.from_raw(meshgen.bump_channel(args.channel[0], args.channel[1], 2)).arrays()
+        flow = FlowConfig(mach=0.5, cfl=1.5, precision=prec, ordering=order, device=device)
+    else:
+        arrays = Mesh.from_raw(meshgen.bump_box_tets(args.n)).arrays()
+        flow = FlowConfig(mach=0.6, cfl=1.0, precision=prec, ordering=order, device=device)
+    s = EulerSolver(arrays, flow, autotune=args.kernel == 0)
     st = s.run(args.iters, profile_stages=True, stage_kernel=args.kernel)
     print(json.dumps({"mode": "profile", "cells": int(arrays["n_cells"]), "kernel": args.kernel,
                       "precision": args.precision, "autotune_ms": s.info()["variant_ms"],
