@@ -103,6 +103,7 @@ SIGNATURES = {
     "e3d_solver_rms_history": (C.c_int, [C.c_void_p, _dp, C.c_int32, C.POINTER(C.c_int32)]),
     "e3d_solver_run_noalloc": (C.c_int, [C.c_void_p, C.POINTER(RunParams), C.POINTER(RunStats), _dp, C.c_int32]),
     "e3d_solver_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int32]),
+    "e3d_fast_reciprocals": (C.c_int, [C.c_int32, _dp, C.c_int64, _dp]),
     "e3d_solver_residual": (C.c_int, [C.c_void_p, _dp, _dp]),
     "e3d_solver_coefficients": (C.c_int, [C.c_void_p, _dp, _dp]),
     "e3d_solver_coefficient_history": (C.c_int, [C.c_void_p, _dp, C.c_int32, C.POINTER(C.c_int32)]),

@@ -1488,6 +1488,21 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
     });
 }
 
+e3d_status e3d_fast_reciprocals(int32_t device, const double *x, int64_t n, double *out) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && (!x || !out))) throw Error(E3D_ERR_INVALID_ARG, "NULL argument or negative count");
+        if (n == 0) return;
+        E3D_CUDA(cudaSetDevice(device));
+        DevBuf<double> dx, dout;
+        dx.alloc((size_t)n);
+        dout.alloc(4 * (size_t)n);
+        E3D_CUDA(cudaMemcpy(dx.p, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+        launch_fast_reciprocals(dx.p, n, dout.p, 0);
+        E3D_CUDA(cudaGetLastError());
+        E3D_CUDA(cudaMemcpy(out, dout.p, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
 e3d_status e3d_solver_set_wait_limit(e3d_solver *solver, int32_t polls) {
     return guarded([&] {
         if (!solver) throw Error(E3D_ERR_INVALID_ARG, "NULL solver");

@@ -25,6 +25,7 @@ constexpr int kStageVariants = 5;
 constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
 void launch_update_exact(const StageArgs &a, cudaStream_t s);
+void launch_fast_reciprocals(const double *x, int64_t n, double *out, cudaStream_t s);
 void launch_update_fast(const StageArgs &a, cudaStream_t s);
 void prepare_batch_exact(size_t smem_bytes, size_t ws_smem_bytes);
 void prepare_batch_fast(size_t smem_bytes, size_t ws_smem_bytes);

@@ -154,6 +154,14 @@ __device__ __forceinline__ void store_prim(double2 *__restrict__ q, int c, const
     q[3 * c + 2] = make_double2(s.p, s.H);
 }
 
+// store_prim with streaming stores (st.global.cs): a stage's new states are read back only by the
+// next stage, after far more traffic than L2 holds on large meshes.
+__device__ __forceinline__ void store_prim_cs(double2 *__restrict__ q, int c, const Prim &s) {
+    __stcs(q + 3 * c, make_double2(s.rho, s.u));
+    __stcs(q + 3 * c + 1, make_double2(s.v, s.w));
+    __stcs(q + 3 * c + 2, make_double2(s.p, s.H));
+}
+
 // ------------------------------------------------------------------------------ fast reciprocals
 // FP64 path only (never FP64_EXACT): reciprocal and reciprocal square root from the single-
 // precision hardware approximations (PTX rcp.approx.ftz.f32 / rsqrt.approx.ftz.f32, relative error
@@ -164,16 +172,19 @@ __device__ __forceinline__ void store_prim(double2 *__restrict__ q, int c, const
 // arguments and seed errors the results were within 1 (reciprocal) and 2 (reciprocal square root)
 // units in the last place of the correctly rounded values, where two Newton-Raphson steps (each
 // squares the error; Markstein, IBM J. Res. Dev. 34, 1990) gave up to 3, with a longer dependency
-// chain and more operations.  Arguments outside [1e-30, 1e30] (where the single-precision seed would flush or
-// overflow), zero, NaN and Inf take the IEEE double operation instead.
-__device__ __forceinline__ bool seed_range(double x) {
-    const double ax = fabs(x);
-    return ax > 1e-30 && ax < 1e30;
+// chain and more operations.  The seed is used when the single-precision argument lies in
+// [2^-99, 2^99) (its bits, sign included, between 0x0E000000 and 0x71000000: one integer compare
+// instead of two double-precision ones), so that seed and result are normal floats; anything else
+// (zero, tiny or huge magnitudes, negative arguments of the square root, NaN and Inf) takes the IEEE
+// double operation.
+__device__ __forceinline__ bool seed_ok(float xf) {
+    return __float_as_uint(xf) - 0x0E000000u < 0x63000000u;
 }
 
 __device__ __forceinline__ double rcp_nr(double x) {
-    if (!seed_range(x)) return 1.0 / x;
-    float xf = (float)x, yf;
+    const float xf = (float)x;
+    if (!seed_ok(fabsf(xf))) return 1.0 / x;
+    float yf;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
     const double y = (double)yf;
     const double e = fma(-x, y, 1.0);
@@ -181,8 +192,9 @@ __device__ __forceinline__ double rcp_nr(double x) {
 }
 
 __device__ __forceinline__ double rsqrt_nr(double x) {
-    if (!(x > 1e-30 && x < 1e30)) return rsqrt(x);
-    float xf = (float)x, yf;
+    const float xf = (float)x;
+    if (!seed_ok(xf)) return rsqrt(x);
+    float yf;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
     const double y = (double)yf;
     const double e = fma(-(x * y), y, 1.0);
@@ -578,23 +590,23 @@ __device__ __forceinline__ double finish_cell(const StageArgs &a, int c, const P
         s.p = (g - 1.0) * fma(-0.5, fma(W[1], s.u, fma(W[2], s.v, W[3] * s.w)), W[4]);
         s.H = (W[4] + s.p) * ir;
     }
-    store_prim(a.qout, c, s);
+    store_prim_cs(a.qout, c, s);
     if (!a.last_stage) return 0.0;
     const size_t st = (size_t)a.w0_stride;
     if (a.integrator == E3D_INTEGRATOR_EULER) {  // the conservative state itself carries over
 #pragma unroll
-        for (int k = 0; k < 5; k++) a.w0[k * st + c] = W[k];
-        a.ecell[c] = E;
+        for (int k = 0; k < 5; k++) __stcs(a.w0 + k * st + c, W[k]);
+        __stcs(a.ecell + c, E);
         if (a.rsq) a.rsq[a.new2old[c]] = R[0] * R[0];
         return R[0] * R[0];
     }
     // the next step's W0 from the primitives (EulerSolver.cpp:431-438)
-    a.w0[0 * st + c] = s.rho;
-    a.w0[1 * st + c] = s.u * s.rho;
-    a.w0[2 * st + c] = s.v * s.rho;
-    a.w0[3 * st + c] = s.w * s.rho;
-    a.w0[4 * st + c] = E * s.rho;
-    a.ecell[c] = E;
+    __stcs(a.w0 + 0 * st + c, s.rho);
+    __stcs(a.w0 + 1 * st + c, s.u * s.rho);
+    __stcs(a.w0 + 2 * st + c, s.v * s.rho);
+    __stcs(a.w0 + 3 * st + c, s.w * s.rho);
+    __stcs(a.w0 + 4 * st + c, E * s.rho);
+    __stcs(a.ecell + c, E);
     if (a.rsq) a.rsq[a.new2old[c]] = R[0] * R[0];
     return R[0] * R[0];
 }
@@ -702,6 +714,25 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
+// L2 policy for data a stage reads once (face records, contribution lists): the lines it brings in
+// are the first to be replaced, so that the state rows neighbouring tiles re-read as halo cells stay
+// in L2 longer.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// bulk_g2s under an L2 cache policy.
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
 // Bulk prefetch of a global range into L2 (16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
@@ -765,9 +796,10 @@ __device__ __forceinline__ void tile_issue_bulk(const StageArgs &a, int tile, in
     const uint32_t b_cg = (uint32_t)nloc * 32u;
     const uint32_t b_ct = (uint32_t)MC * T * 2u;
     mbar_expect_tx(bar, b_state + b_rec + b_ct);
+    const uint64_t once = l2_evict_first();
     bulk_g2s(b.st, a.qin + 3 * (size_t)c0, b_state, bar);
-    bulk_g2s(b.rec, a.tile_rec + rec_off, b_rec, bar);
-    bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+    bulk_g2s_hint(b.rec, a.tile_rec + rec_off, b_rec, bar, once);
+    bulk_g2s_hint(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar, once);
     for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
     bulk_prefetch_l2(a.cgeo + c0, b_cg);
 }
@@ -841,10 +873,13 @@ __device__ __forceinline__ void tile_fluxes(const StageArgs &a, const TileBuf &b
 }
 
 // W0 and geometry of owned cell i (global memory, prefetched into L2 when the tile started).
+// Streaming loads (ld.global.cs): the stage reads these rows once.
 __device__ __forceinline__ void tile_load_cell(const StageArgs &a, int c0, int i, double W0[5], double4 &cg) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c0 + i];
-    cg = a.cgeo[c0 + i];
+    for (int k = 0; k < 5; k++) W0[k] = __ldcs(a.w0 + (size_t)k * a.w0_stride + c0 + i);
+    const double2 *g = reinterpret_cast<const double2 *>(a.cgeo + c0 + i);
+    const double2 g0 = __ldcs(g), g1 = __ldcs(g + 1);
+    cg = make_double4(g0.x, g0.y, g1.x, g1.y);
 }
 
 // Cell i of the tile: sum of its contributions, then time step and update; returns R_rho^2 on

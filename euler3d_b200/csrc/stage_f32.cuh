@@ -31,8 +31,8 @@ __device__ __forceinline__ float rsqrt_f(float x) {
 __device__ __forceinline__ void make_rec32(float4 *dst, double rho, double u, double v, double w, double p, double H,
                                            double g) {
     const float fr = (float)rho, fp = (float)p;
-    dst[0] = make_float4(fr, (float)u, (float)v, (float)w);
-    dst[1] = make_float4(fp, (float)H, fr * rsqrt_f(fr), rsqrt_f((float)g * fp * fr));
+    __stcs(dst, make_float4(fr, (float)u, (float)v, (float)w));  // streaming stores, as store_prim_cs
+    __stcs(dst + 1, make_float4(fp, (float)H, fr * rsqrt_f(fr), rsqrt_f((float)g * fp * fr)));
 }
 
 // Roe flux with Harten's fix (Solver::Roe, src/solver/ConvectiveFluxesSchemes.cpp:10-165) in single
@@ -178,8 +178,8 @@ __device__ __forceinline__ void tile_fluxes_f32(const StageArgs &a, const Tile32
 // The owner's W0 and geometry (global memory, prefetched into L2 when the tile started).
 __device__ __forceinline__ void tile_load_cell_f32(const StageArgs &a, int c, double W0[5], float4 &cg) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) W0[k] = a.w0[(size_t)k * a.w0_stride + c];
-    cg = a.cgeo32[c];
+    for (int k = 0; k < 5; k++) W0[k] = __ldcs(a.w0 + (size_t)k * a.w0_stride + c);  // read once: streaming
+    cg = __ldcs(a.cgeo32 + c);
 }
 
 // Cell i of the tile: sum of its faces' F*S, time step and update; returns R_rho^2 on the last stage.
@@ -226,8 +226,8 @@ __device__ __forceinline__ double tile_update_f32(const StageArgs &a, const Tile
     // the conservative state carries over exactly in double
     const size_t sd = (size_t)a.w0_stride;
 #pragma unroll
-    for (int k = 0; k < 5; k++) a.w0[k * sd + c] = W[k];
-    a.ecell[c] = W[4] * ir;
+    for (int k = 0; k < 5; k++) __stcs(a.w0 + k * sd + c, W[k]);
+    __stcs(a.ecell + c, W[4] * ir);
     return R[0] * R[0];
 }
 
@@ -261,8 +261,9 @@ __device__ __forceinline__ void tile_body_f32(const StageArgs &a, int tile, doub
         const uint32_t b_ct = (uint32_t)MC * T * 2u;
         mbar_expect_tx(bar, b_state + b_rec + b_ct);
         bulk_g2s(b.st, a.q32in + 2 * (size_t)c0, b_state, bar);
-        bulk_g2s(b.rec, a.tile_rec32 + rec_off, b_rec, bar);
-        bulk_g2s(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar);
+        const uint64_t once = l2_evict_first();
+        bulk_g2s_hint(b.rec, a.tile_rec32 + rec_off, b_rec, bar, once);
+        bulk_g2s_hint(b.ct, a.tile_contrib + (size_t)tile * MC * T, b_ct, bar, once);
         for (int k = 0; k < 5; k++) bulk_prefetch_l2(a.w0 + (size_t)k * a.w0_stride + c0, b_w0);
         bulk_prefetch_l2(a.cgeo32 + c0, b_cg);
     }

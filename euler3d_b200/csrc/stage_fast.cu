@@ -32,6 +32,23 @@ void launch_batch_ws_fast(const BatchStage &bs, int grid, size_t smem_bytes, cud
     tile_ws_batch_kernel<WS_FAST><<<grid, kWsThreads, smem_bytes, s>>>(bs);
 }
 
+// The FP64 mode's reciprocal and reciprocal square root beside CUDA's own double-precision
+// operations, for their accuracy check: out[4 i .. 4 i + 3] = rcp_nr(x), 1.0 / x, rsqrt_nr(x), rsqrt(x).
+__global__ void fast_reciprocals_kernel(const double *__restrict__ x, int64_t n, double *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        out[4 * i] = rcp_nr(v);
+        out[4 * i + 1] = 1.0 / v;
+        out[4 * i + 2] = rsqrt_nr(v);
+        out[4 * i + 3] = rsqrt(v);
+    }
+}
+
+void launch_fast_reciprocals(const double *x, int64_t n, double *out, cudaStream_t s) {
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    fast_reciprocals_kernel<<<blocks, 256, 0, s>>>(x, n, out);
+}
+
 // variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;
 // 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and warp-specialised;
 // 4: face tiles with registers for 7 blocks/SM

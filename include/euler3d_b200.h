@@ -273,6 +273,13 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *para
  * has no device waits. */
 e3d_status e3d_solver_set_wait_limit(e3d_solver *solver, int32_t polls);
 
+/* Accuracy check of the FP64 mode's fast reciprocal and reciprocal square root (single-precision
+ * seed, one series refinement step): for the n arguments x (host memory) writes, to out (host,
+ * 4 n doubles), out[4 i] = the FP64 mode's 1/x, out[4 i + 1] = CUDA's 1.0 / x, out[4 i + 2] = the
+ * FP64 mode's 1/sqrt(x) and out[4 i + 3] = CUDA's rsqrt(x), evaluated on `device`.  No counterpart
+ * in the reference, whose solver divides and takes square roots in IEEE double precision. */
+e3d_status e3d_fast_reciprocals(int32_t device, const double *x, int64_t n, double *out);
+
 /* Density RMS of every iteration of the last e3d_solver_run (the residuals.dat column). */
 e3d_status e3d_solver_rms_history(e3d_solver *solver, double *out, int32_t capacity, int32_t *count);
 
