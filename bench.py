@@ -386,9 +386,11 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (state + mesh ~3 GB per replica)", "setup_s": round(setup_s, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (tr * n_cells if tr else None), "peak_kind": peak_kind,
-                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_ws_kernel<WS_F32>", "tile_kernel_f32<8>"] if args.precision == "fp32" else
+                     "kernel": (["-", "-", "tile_kernel_f32<4>", "tile_ws_kernel<WS_F32>", "tile_kernel_f32<8>", "-", "-"]
+                                if args.precision == "fp32" else
                                 ["stage_kernel<false,4>", "stage_kernel<false,5>", "tile_kernel<false,4>",
-                                 "tile_ws_kernel<WS_FAST>", "tile_kernel<false,7>"])[solver.info()["stage_variant"]],
+                                 "tile_ws_kernel<WS_FAST>", "tile_kernel<false,7>", "colour_kernel<128> (per class)",
+                                 "colour_kernel<512> (per class)"])[solver.info()["stage_variant"]],
                      "bytes_per_cell_stage": bytes_per_cell,
                      "avg_launch_ms": stage_ms, "launches_timed": tstats["stage_launches"],
                      "timing": "event pairs around every stage kernel in a second run of the timed graph",

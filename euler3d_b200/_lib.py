@@ -11,12 +11,13 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libeuler3d_b200.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 E3D_OK, E3D_ERR_INVALID_ARG, E3D_ERR_OOM, E3D_ERR_NONFINITE, E3D_ERR_TIMEOUT, E3D_ERR_CUDA, E3D_ERR_MESH = range(7)
 SCHEME_ROE, SCHEME_AUSM = 0, 1
 PREC_FP64_EXACT, PREC_FP64, PREC_FP32_FLUX = 0, 1, 2
 ORDER_NATIVE, ORDER_RCM, ORDER_SPATIAL = 0, 1, 2
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_GATHER_B, KERNEL_TILE, KERNEL_TILE_PIPE, KERNEL_TILE_B3 = 0, 1, 2, 3, 4, 5
+KERNEL_COLOUR, KERNEL_COLOUR_B = 6, 7  # face colouring, 128 / 512 faces per block (FP64)
 STOP_MAX_ITER, STOP_RESIDUAL, STOP_COEFFICIENTS, STOP_STALL = 0, 1, 2, 3
 INTEGRATOR_RK5, INTEGRATOR_EULER = 0, 1
 BATCH_KERNEL_TILES, BATCH_KERNEL_WS = 0, 1
@@ -65,7 +66,7 @@ class RunStats(C.Structure):
 
 class SolverInfo(C.Structure):
     _fields_ = [("n_cells", C.c_int32), ("n_ghosts", C.c_int32), ("n_faces", C.c_int32),
-                ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 5),
+                ("stage_variant", C.c_int32), ("n_variants", C.c_int32), ("variant_ms", C.c_float * 8),
                 ("tile_smem_bytes", C.c_int32), ("device_bytes", C.c_int64)]
 
 

@@ -558,6 +558,58 @@ static void bank_order(const FaceRec *rec, int n, std::vector<int> &order, std::
     }
 }
 
+// Face-colouring classes (stage variants 5 and 6), from the device's own connectivity: every
+// interior face once (from its left cell's list) and every boundary face, each given the smallest
+// class that neither of its cells has taken yet, visited in device cell order.  A class keeps its
+// faces in that order (ascending left cell), so its state gathers walk memory forwards.  On a mesh
+// whose cells have at most k faces a face meets at most 2k - 2 others, so 2k - 1 classes suffice
+// (11 for hexahedra); 32 are available.
+void build_colours(Solver *S) {
+    if (S->colours_built()) return;
+    const int N = S->N;
+    cudaStream_t s = S->stream;
+    std::vector<int> cptr(N + 1);
+    std::vector<int2> cf(S->cf.n);
+    std::vector<double4> fgeo(S->fgeo.n);
+    E3D_CUDA(cudaMemcpyAsync(cptr.data(), S->cptr.p, cptr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    E3D_CUDA(cudaMemcpyAsync(cf.data(), S->cf.p, cf.size() * sizeof(int2), cudaMemcpyDeviceToHost, s));
+    E3D_CUDA(cudaMemcpyAsync(fgeo.data(), S->fgeo.p, fgeo.size() * sizeof(double4), cudaMemcpyDeviceToHost, s));
+    E3D_CUDA(cudaStreamSynchronize(s));
+    const int mask = (1 << kTagBits) - 1;
+    std::vector<uint32_t> used(N, 0u);
+    std::vector<unsigned char> cls(cf.size(), 0xff);  // class of entry e (0xff: the right cell's entry)
+    int n_cls = 0;
+    std::vector<int> count(33, 0);
+    for (int c = 0; c < N; c++)
+        for (int e = cptr[c]; e < cptr[c + 1]; e++) {
+            const int tag = cf[e].x & mask, idx = cf[e].x >> kTagBits;
+            if (tag == TAG_RIGHT) continue;
+            const bool inter = tag == TAG_LEFT;
+            const uint32_t busy = used[c] | (inter ? used[idx] : 0u);
+            if (busy == 0xffffffffu) throw Error(E3D_ERR_MESH, "face colouring needs more than 32 classes");
+            const int k = __builtin_ctz(~busy);
+            used[c] |= 1u << k;
+            if (inter) used[idx] |= 1u << k;
+            cls[e] = (unsigned char)k;
+            count[k + 1]++;
+            n_cls = std::max(n_cls, k + 1);
+        }
+    for (int k = 0; k < 32; k++) count[k + 1] += count[k];
+    std::vector<ColourFace> faces(count[n_cls]);
+    std::vector<int> head(count.begin(), count.begin() + n_cls);
+    for (int c = 0; c < N; c++)
+        for (int e = cptr[c]; e < cptr[c + 1]; e++) {
+            if (cls[e] == 0xff) continue;
+            const double4 g = fgeo[cf[e].y];
+            faces[head[cls[e]]++] = ColourFace{c, cf[e].x >> kTagBits, cf[e].x & mask, 0, g.x, g.y, g.z, g.w};
+        }
+    S->colour_ptr.assign(count.begin(), count.begin() + n_cls + 1);
+    S->n_colours = n_cls;
+    S->colour_faces.upload(faces, s);
+    S->colour_r.alloc(3 * (size_t)N);
+    E3D_CUDA(cudaStreamSynchronize(s));
+}
+
 // Face tiles for tile_kernel.  Tile t owns cells [t*T, t*T + T); its local cells are the owned
 // ones followed by the halo (outside neighbours, ascending); its faces are every interior face with
 // an owned cell (once, interior ones before boundary ones) and its owned cells' boundary faces; each
@@ -1291,6 +1343,7 @@ e3d_status e3d_solver_run(e3d_solver *solver, const e3d_run_params *rp, e3d_run_
             const int v = rp->stage_kernel - 1;
             if (!S->variant_ok(v))
                 throw Error(E3D_ERR_INVALID_ARG, "stage kernel variant not available for this mesh and precision");
+            if (v >= kColourVariant) build_colours(S);
             if (S->f32) prepare_tile_f32(S->tile32_smem, S->pipe_smem);
             else if (v >= 2 && S->prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(S->tile_smem, S->pipe_smem);
             else if (v >= 2) prepare_tile_fast(S->tile_smem, S->pipe_smem);
@@ -1493,13 +1546,19 @@ e3d_status e3d_fast_reciprocals(int32_t device, const double *x, int64_t n, doub
         if (n < 0 || (n > 0 && (!x || !out))) throw Error(E3D_ERR_INVALID_ARG, "NULL argument or negative count");
         if (n == 0) return;
         E3D_CUDA(cudaSetDevice(device));
-        DevBuf<double> dx, dout;
-        dx.alloc((size_t)n);
-        dout.alloc(4 * (size_t)n);
-        E3D_CUDA(cudaMemcpy(dx.p, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
-        launch_fast_reciprocals(dx.p, n, dout.p, 0);
+        struct Bufs {  // released on every exit
+            DevBuf<double> x, out;
+            ~Bufs() {
+                x.release();
+                out.release();
+            }
+        } d;
+        d.x.alloc((size_t)n);
+        d.out.alloc(4 * (size_t)n);
+        E3D_CUDA(cudaMemcpy(d.x.p, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+        launch_fast_reciprocals(d.x.p, n, d.out.p, 0);
         E3D_CUDA(cudaGetLastError());
-        E3D_CUDA(cudaMemcpy(out, dout.p, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+        E3D_CUDA(cudaMemcpy(out, d.out.p, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }
 

@@ -19,8 +19,14 @@ void prepare_tile_exact(size_t smem_bytes, size_t pipe_smem_bytes);
 void prepare_tile_fast(size_t smem_bytes, size_t pipe_smem_bytes);
 void launch_stage_f32(const StageArgs &a, cudaStream_t s, int variant);
 void prepare_tile_f32(size_t smem_bytes, size_t ws_smem_bytes);
-// gather (two register budgets), face tiles, warp-specialised persistent face tiles, face tiles at 7 blocks/SM
-constexpr int kStageVariants = 5;
+// gather (two register budgets), face tiles, warp-specialised persistent face tiles, face tiles at 7 blocks/SM,
+// face colouring at 128 and at 512 faces per block
+constexpr int kStageVariants = 7;
+constexpr int kColourVariant = 5;  // variants 5 and 6
+void launch_colour_fast(const StageArgs &a, const ColourFace *faces, int n, double2 *rc, int per_block, cudaStream_t s);
+void launch_colour_finish_fast(const StageArgs &a, const double2 *rc, cudaStream_t s);
+struct Solver;
+void build_colours(Solver *S);
 
 constexpr int kReduceThreads = 256;
 constexpr int kCoeffThreads = 512;
@@ -192,6 +198,7 @@ struct Solver {
         tile_rec32.release();
         tile_rec32_off.release();
         tile_contrib.release();
+        release_colours();
         cf.release();
         fgeo.release();
         cgeo.release();
@@ -213,6 +220,22 @@ struct Solver {
 
     int64_t state_size() const { return (int64_t)N + G; }
 
+    // Face colouring (variants 5 and 6, FP64 mode): the faces grouped in classes that share no cell,
+    // class k at [colour_ptr[k], colour_ptr[k + 1]), and the residual accumulator.  Built on first
+    // use (build_colours), released when the autotuner picks another variant.
+    DevBuf<ColourFace> colour_faces;
+    std::vector<int> colour_ptr;
+    DevBuf<double2> colour_r;  // 3 per cell
+    int n_colours = 0;
+    void release_colours() {
+        colour_faces.release();
+        colour_r.release();
+        colour_faces.n = colour_r.n = 0;
+        colour_ptr.clear();
+        n_colours = 0;
+    }
+    bool colours_built() const { return colour_faces.p != nullptr; }
+
     int64_t device_bytes() const {
         return (int64_t)(cptr.n + new2old_d.n + ghost_ref_d.n + wall_cell.n + tile_halo_ptr.n + tile_halo.n +
                          tile_face_ptr.n) * 4 + (int64_t)cf.n * 8 + (int64_t)tile_rec.n * 40 + (int64_t)tile_rec_off.n * 8 +
@@ -221,7 +244,8 @@ struct Solver {
                (int64_t)(fgeo.n + cgeo.n) * 32 + (int64_t)(q[0].n + q[1].n) * 16 +
                (int64_t)(w0.n + ecell.n + minit.n + ghost.n + partials.n + staging.n + wall_svec.n + wall_center.n +
                          hist.n + scratch.n + den.n + rbuf.n + smooth_flags.n + samples.n + wall_cp.n + rsq.n) * 8 +
-               (int64_t)(nb_ptr.n + nb.n) * 4 + (int64_t)sizeof(Control);
+               (int64_t)(nb_ptr.n + nb.n) * 4 + (int64_t)colour_faces.n * 48 + (int64_t)colour_r.n * 16 +
+               (int64_t)sizeof(Control);
     }
 
     StageArgs stage_args(int in_buf, double alpha, int first, int last) {
@@ -288,11 +312,24 @@ struct Solver {
         if (v == 2) return tiles_ok;
         if (v == 3) return pipe_ok;
         if (v == 4) return tiles_ok && prm.precision == E3D_PREC_FP64;
+        if (v >= kColourVariant) return prm.precision == E3D_PREC_FP64;
         return true;
     }
 
+    // The launches of one stage with variant v (face colouring: one per class and the update).
+    int stage_launches(int v) const { return v >= kColourVariant ? n_colours + 1 : 1; }
+
     void launch_stage(const StageArgs &a, int v = -1) {
         if (v < 0) v = variant;
+        if (v >= kColourVariant) {  // the accumulator is cleared, every class adds, the update reads it
+            E3D_CUDA(cudaMemsetAsync(colour_r.p, 0, colour_r.n * sizeof(double2), stream));
+            const int per_block = v == kColourVariant ? 128 : 512;
+            for (int k = 0; k < n_colours; k++)
+                launch_colour_fast(a, colour_faces.p + colour_ptr[k], colour_ptr[k + 1] - colour_ptr[k], colour_r.p,
+                                   per_block, stream);
+            launch_colour_finish_fast(a, colour_r.p, stream);
+            return;
+        }
         if (f32) launch_stage_f32(a, stream, v);
         else if (prm.precision == E3D_PREC_FP64_EXACT) launch_stage_exact(a, stream, v);
         else launch_stage_fast(a, stream, v);
@@ -316,6 +353,7 @@ struct Solver {
             if (prm.precision == E3D_PREC_FP64_EXACT) prepare_tile_exact(tile_smem, pipe_smem);
             else prepare_tile_fast(tile_smem, pipe_smem);
         }
+        if (variant_ok(kColourVariant)) build_colours(this);
         for (int v = 0; v < kStageVariants; v++) {
             variant_ms[v] = -1.0f;
             if (!variant_ok(v)) continue;
@@ -334,6 +372,10 @@ struct Solver {
         }
         E3D_CUDA(cudaGetLastError());
         ghost_copy.release();
+        if (variant < kColourVariant) {
+            E3D_CUDA(cudaStreamSynchronize(stream));
+            release_colours();
+        }
     }
 
     // Without tuning: the face-tile kernel (seven blocks per SM in FP64, eight in FP32_FLUX), or the
@@ -389,7 +431,7 @@ struct Solver {
     bool euler() const { return prm.integrator == E3D_INTEGRATOR_EULER; }
     // Stages per iteration (RK5: 5; explicit Euler: 1) and kernels per stage and per iteration.
     int n_stages() const { return euler() ? 1 : 5; }
-    int kernels_per_stage() const { return smoothing ? 4 : 1; }
+    int kernels_per_stage() const { return stage_launches(variant) + (smoothing ? 3 : 0); }
     int kernels_per_iteration() const { return n_stages() * kernels_per_stage() + 2; }
 
     // Stage s of an iteration from q[b] (EulerSolver::RungeKutta, src/solver/EulerSolver.cpp:425-472,

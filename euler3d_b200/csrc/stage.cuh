@@ -683,6 +683,102 @@ __global__ void __launch_bounds__(kStageThreads, MINB) stage_kernel(StageArgs a)
     if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
 }
 
+// ------------------------------------------------------------------------------ face colouring
+// FP64 mode only.  The faces are split into colour classes in which no two faces share a cell.  One
+// launch per class evaluates each face once and adds its F*S to the residuals of its cells in
+// global memory (the left cell's plus, the right cell's minus) with no atomics: within a class every
+// cell receives at most one contribution.  A last kernel runs the time step and the update from the
+// accumulated residuals.  Each cell sums its faces in class order, a fixed order, so the results are
+// deterministic; it is not the reference's face order, so FP64_EXACT never takes this path.
+struct ColourFace {
+    int l;          // interior cell (device index): the face's left cell
+    int r;          // right cell (interior face) or ghost index (boundary face)
+    int tag;        // TAG_LEFT for an interior face, else the boundary class
+    int pad;
+    double nx, ny, nz, S;  // unit normal (from l to r) and area
+};
+static_assert(sizeof(ColourFace) == 48, "ColourFace layout");
+
+// The residual accumulator: one 48-byte record per cell (R0..R4 and a pad), so that the update of
+// a scattered cell moves two 32-byte sectors instead of five.
+__device__ __forceinline__ void colour_add(double2 *__restrict__ rc, int c, const double F[5], double S, bool plus) {
+    double2 *r = rc + 3 * (size_t)c;
+    double2 r0 = r[0], r1 = r[1], r2 = r[2];
+    if (plus) {
+        r0.x += F[0] * S;
+        r0.y += F[1] * S;
+        r1.x += F[2] * S;
+        r1.y += F[3] * S;
+        r2.x += F[4] * S;
+    } else {
+        r0.x -= F[0] * S;
+        r0.y -= F[1] * S;
+        r1.x -= F[2] * S;
+        r1.y -= F[3] * S;
+        r2.x -= F[4] * S;
+    }
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+
+// One face per thread over class [f, f + n); rc is the residual accumulator (3 double2 per cell).
+template <int NT>
+__global__ void __launch_bounds__(NT) colour_kernel(StageArgs a, const ColourFace *__restrict__ f, int n,
+                                                    double2 *__restrict__ rc) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    const int i = blockIdx.x * NT + threadIdx.x;
+    if (i >= n) return;
+    const ColourFace cf = f[i];
+    const double g = a.gamma;
+    const double4 fg = make_double4(cf.nx, cf.ny, cf.nz, cf.S);
+    const Prim L = load_prim(a.qin, cf.l);
+    double F[5];
+    if (cf.tag == TAG_LEFT) {
+        const Prim R = load_prim(a.qin, cf.r);
+        if (a.scheme == 1)
+            ausm_fast(L, R, rsqrt_nr(g * L.p * L.rho), rsqrt_nr(g * R.p * R.rho), fg.x, fg.y, fg.z, g, F);
+        else
+            roe_fast(L, R, L.rho * rsqrt_nr(L.rho), R.rho * rsqrt_nr(R.rho), rsqrt_nr(g * L.p * L.rho), fg.x, fg.y,
+                     fg.z, g, F);
+        colour_add(rc, cf.l, F, fg.w, true);
+        colour_add(rc, cf.r, F, fg.w, false);
+        return;
+    }
+    Prim gs;
+    if (boundary_face(a, cf.tag, a.ghost + 8 * (size_t)cf.r, cf.l, L, fg, F, gs)) {
+        // symmetry ghost: rho and p are the cell's
+        const double rl = rsqrt_nr(g * L.p * L.rho);
+        if (a.scheme == 1) ausm_fast(L, gs, rl, rl, fg.x, fg.y, fg.z, g, F);
+        else {
+            const double sl = L.rho * rsqrt_nr(L.rho);
+            roe_fast(L, gs, sl, sl, rl, fg.x, fg.y, fg.z, g, F);
+        }
+    }
+    colour_add(rc, cf.l, F, fg.w, true);
+}
+
+// After the last class: time step and update of every cell from its accumulated residual (the
+// update, the split residual phase or the residual-only output, as finish_cell does for the other
+// stage kernels), RMS partials per block of kStageThreads cells.
+template <int = 0>  // instantiated in the FP64 translation unit only
+__global__ void __launch_bounds__(kStageThreads) colour_finish_kernel(StageArgs a, const double2 *__restrict__ rc) {
+    if (!a.residual_only && a.ctl->done) return;  // uniform across the grid
+    const int c = blockIdx.x * kStageThreads + threadIdx.x;
+    double r2 = 0.0;
+    if (c < a.n_cells) {
+        const Prim me = load_prim(a.qin, c);
+        const size_t st = (size_t)a.w0_stride;
+        const double2 r0 = rc[3 * (size_t)c], r1 = rc[3 * (size_t)c + 1], r2v = rc[3 * (size_t)c + 2];
+        const double R[5] = {r0.x, r0.y, r1.x, r1.y, r2v.x};
+        double W0[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) W0[k] = a.w0[k * st + c];
+        r2 = finish_cell<false>(a, c, me, rsqrt_nr(a.gamma * me.p * me.rho), R, W0, a.cgeo[c]);
+    }
+    if (a.last_stage && !a.residual_only) block_sum_store(r2, a.partials + blockIdx.x);
+}
+
 // ------------------------------------------------------------------------------ async copies
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 

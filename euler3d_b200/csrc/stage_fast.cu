@@ -49,6 +49,19 @@ void launch_fast_reciprocals(const double *x, int64_t n, double *out, cudaStream
     fast_reciprocals_kernel<<<blocks, 256, 0, s>>>(x, n, out);
 }
 
+// One colour class of a face-colouring stage: n faces, `per_block` (128 or 512) faces per block.
+void launch_colour_fast(const StageArgs &a, const ColourFace *faces, int n, double2 *rc, int per_block,
+                        cudaStream_t s) {
+    if (n <= 0) return;
+    if (per_block == 512) colour_kernel<512><<<(n + 511) / 512, 512, 0, s>>>(a, faces, n, rc);
+    else colour_kernel<128><<<(n + 127) / 128, 128, 0, s>>>(a, faces, n, rc);
+}
+
+// The update after the last colour class.
+void launch_colour_finish_fast(const StageArgs &a, const double2 *rc, cudaStream_t s) {
+    colour_finish_kernel<><<<(a.n_cells + kStageThreads - 1) / kStageThreads, kStageThreads, 0, s>>>(a, rc);
+}
+
 // variant 0: gather kernel, registers for 4 blocks/SM; 1: gather kernel, 5 blocks/SM;
 // 2: face tiles, one block per tile (4 blocks/SM); 3: face tiles, persistent and warp-specialised;
 // 4: face tiles with registers for 7 blocks/SM

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define E3D_ABI_VERSION 2
+#define E3D_ABI_VERSION 3
 
 typedef enum e3d_status {
 	E3D_OK = 0,
@@ -177,14 +177,16 @@ e3d_status e3d_solver_create(const e3d_mesh_desc *mesh, const e3d_flow_params *p
 void e3d_solver_destroy(e3d_solver *solver);
 
 /* What the handle holds on the device and what its autotuner chose.  At creation the solver times
- * each compiled variant of the stage kernel (register budget / occupancy) on this mesh, with
- * writes redirected to scratch, and keeps the fastest. */
+ * each stage-kernel variant available for its precision on this mesh -- per-cell gather and face
+ * tiles at several register budgets (occupancies), the persistent face-tile kernel, and face
+ * colouring at two block sizes (faces per block) -- with writes redirected to scratch, and keeps the
+ * fastest. */
 typedef struct e3d_solver_info {
 	int32_t n_cells, n_ghosts, n_faces;
 	int32_t stage_variant;            /* variant in use */
 	int32_t n_variants;
-	float variant_ms[5];              /* measured duration of one stage launch per variant (-1: not
-	                                     available for this mesh and precision) */
+	float variant_ms[8];              /* measured duration of one stage per variant, n_variants of
+	                                     them (-1: not available for this mesh and precision) */
 	int32_t tile_smem_bytes;          /* dynamic shared memory of one face-tile block (0: no tiles) */
 	int64_t device_bytes;             /* device memory held by the handle */
 } e3d_solver_info;
@@ -215,7 +217,9 @@ typedef struct e3d_run_params {
 	                                     register budgets (FP64 modes); 3: face tiles; 4: persistent
 	                                     face tiles with a producer warp streaming tiles to consumer
 	                                     warps; 5: face tiles at seven blocks per SM (FP64) or eight
-	                                     (FP32_FLUX) (kept for later runs) */
+	                                     (FP32_FLUX); 6, 7: face colouring, one launch per class of
+	                                     faces that share no cell, 128 or 512 faces per block (FP64)
+	                                     (kept for later runs) */
 	double min_residual_drop;         /* > 0: also stop once the density RMS is below this fraction of
 	                                     the run's first RMS (a relative tolerance such as 1e-8); 0 off.
 	                                     No counterpart in the reference, whose test is absolute. */

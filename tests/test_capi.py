@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_status_strings():
     lib = _lib.load()
-    assert lib.e3d_abi_version() == _lib.ABI_VERSION == 2
+    assert lib.e3d_abi_version() == _lib.ABI_VERSION == 3
     assert lib.e3d_status_string(_lib.E3D_ERR_NONFINITE) == b"non-finite solution"
 
 

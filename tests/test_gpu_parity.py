@@ -252,12 +252,13 @@ def test_autotune_info():
     name = "tets"
     s = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL))
     info = s.info()
-    assert len(info["variant_ms"]) == 5 and 0 <= info["stage_variant"] < 5
-    assert all(t > 0 for t in info["variant_ms"])  # FP64: every variant runs on this mesh
+    assert len(info["variant_ms"]) == 7 and 0 <= info["stage_variant"] < 7
+    assert all(t > 0 for t in info["variant_ms"])  # FP64: every variant runs on this mesh, colouring included
     assert info["variant_ms"][info["stage_variant"]] == min(info["variant_ms"])
     assert 0 < info["tile_smem_bytes"] <= 227 * 1024
     exact = EulerSolver(prepared(name), CASES[name].flow(ordering=_lib.ORDER_SPATIAL, precision=_lib.PREC_FP64_EXACT))
-    assert exact.info()["variant_ms"][4] == -1.0  # no seven-blocks-per-SM tile kernel in exact mode
+    # no seven-blocks-per-SM tile kernel and no colouring (another summation order) in exact mode
+    assert exact.info()["variant_ms"][4:] == [-1.0, -1.0, -1.0]
 
 
 # ------------------------------------------------------------------ FP32_FLUX mode
