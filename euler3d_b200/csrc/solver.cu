@@ -1513,7 +1513,7 @@ e3d_status e3d_solver_run_noalloc(e3d_solver *solver, const e3d_run_params *rp, 
             launch_finalize(S->finalize_args(partials, hist), S->stream);
             launch_coeff(S->coeff_args(b, 1, nullptr), S->stream);
             E3D_CUDA(cudaGetLastError());
-            launches += 7;
+            launches += 5 * S->stage_launches(S->variant) + 2;
             if ((it + 1) % every == 0 || it + 1 == max_iter) {
                 E3D_CUDA(cudaMemcpyAsync(S->ctl_host, S->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S->stream));
                 E3D_CUDA(cudaStreamSynchronize(S->stream));

@@ -40,6 +40,24 @@ def test_noalloc_run_matches_run(name, precision):
         assert np.array_equal(new.wall_cp(), ref.wall_cp())
 
 
+def test_noalloc_with_colouring():
+    """A handle whose stage kernel is the face-colouring variant (chosen by an earlier run) runs it
+    allocation-free too: its classes and accumulator were built when the variant was chosen."""
+    name = "tets"
+    flow = CASES[name].flow(precision=_lib.PREC_FP64, ordering=_lib.ORDER_SPATIAL)
+    ref = EulerSolver(prepared(name), flow)
+    new = EulerSolver(prepared(name), flow)
+    ref.run(0, stage_kernel=_lib.KERNEL_COLOUR)
+    new.run(0, stage_kernel=_lib.KERNEL_COLOUR)
+    st_ref = ref.run(7)
+    st_new, hist_new = new.run_noalloc(7)
+    assert st_new["iterations"] == st_ref["iterations"] == 7
+    assert np.array_equal(hist_new, ref.rms_history())
+    a, b = ref.get_state(), new.get_state()
+    for k in STATE_KEYS:
+        assert np.array_equal(a[k], b[k]), k
+
+
 def test_noalloc_leaves_no_stale_records(tmp_path):
     """After an allocation-free run the handle holds no RMS history or coefficient samples of it, so
     the queries of them must not hand back an earlier e3d_solver_run's records as this run's."""
