@@ -63,8 +63,9 @@ def parse():
     ap.add_argument("--iters", type=int, default=2, help="profile mode: RK5 iterations")
     ap.add_argument("--channel", type=int, nargs=2, default=None, metavar=("NX", "NY"),
                     help="profile mode: a 2-layer bump channel of NX x NY x 2 hexahedra instead of the tetrahedral box")
-    ap.add_argument("--ref-mesh", choices=["c3", "c1"], default="c3",
-                    help="reference arm: the bench mesh (c3) or the 64x32x2 bump channel of config 1 (Mach 0.5, CFL 1.5)")
+    ap.add_argument("--ref-mesh", choices=["c3", "c1", "c2"], default="c3",
+                    help="reference arm: the bench mesh (c3), the 64x32x2 bump channel of config 1 (Mach 0.5, "
+                         "CFL 1.5) or the 256x128x4 biconvex O-grid of config 2 (Mach 0.8, AoA 1.25, CFL 1.2)")
     ap.add_argument("--ref-ranks", type=int, default=0, help="reference arm: MPI ranks (0: one per host core)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the first iteration against the CPU oracle")
@@ -530,7 +531,8 @@ def host_cores() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
 
 
-def run_reference_mpi(raw, arrays, ranks: int, warm: int, iters: int, mach: float, cfl: float, workdir: str) -> dict:
+def run_reference_mpi(raw, arrays, ranks: int, warm: int, iters: int, mach: float, cfl: float, workdir: str,
+                      aoa: float = 0.0) -> dict:
     """The reference's own solver program on ``ranks`` host cores through its multi-rank path:
     the mesh cut into ``ranks`` x-slab partitions (.par files in the reference's layout), each rank
     one process (shared-memory MPI), EulerSolver::Run timed by the driver over ``iters`` iterations
@@ -539,7 +541,7 @@ def run_reference_mpi(raw, arrays, ranks: int, warm: int, iters: int, mach: floa
 
     pattern = os.path.join(workdir, "part_#.par")
     meshgen.write_partitions(raw, ranks, pattern, arrays=arrays)
-    cfg = meshgen.CaseConfig(mach=mach, aoa=0.0, cfl=cfl, max_iter=iters, sampling=1_000_000_000)
+    cfg = meshgen.CaseConfig(mach=mach, aoa=aoa, cfl=cfl, max_iter=iters, sampling=1_000_000_000)
     cfg_path = os.path.join(workdir, "case.e3d")
     meshgen.write_e3d(cfg, cfg_path, pattern, os.path.join(workdir, "out.dat"), n_partitions=ranks)
     env = dict(os.environ, E3D_MPI_RANKS=str(ranks))
@@ -561,9 +563,13 @@ def run_reference(args, rank, world):
 
     K, W = args.steps, max(args.warmup, 3)
     cores = host_cores()
+    aoa = 0.0
     if args.ref_mesh == "c1":
         raw, mach, cfl = meshgen.bump_channel(64, 32, 2), 0.5, 1.5
         workload = "bump_channel 64x32x2 (4,096 hexahedra), Mach 0.5, Roe, RK5, CFL 1.5"
+    elif args.ref_mesh == "c2":
+        raw, mach, cfl, aoa = meshgen.biconvex_ogrid(256, 128, 4), 0.8, 1.2, 1.25
+        workload = "biconvex O-grid 256x128x4 (262,144 prisms), Mach 0.8, AoA 1.25, Roe, RK5, CFL 1.2"
     else:
         raw, mach, cfl = meshgen.bump_box_tets(args.n), 0.6, 1.0
         workload = WORKLOAD
@@ -572,7 +578,7 @@ def run_reference(args, rank, world):
         ranks = args.ref_ranks if args.ref_ranks > 0 else max(1, min(cores, 64))
         arrays = Mesh.from_raw(raw).arrays()
         with tempfile.TemporaryDirectory(prefix="e3dref") as d:
-            res = run_reference_mpi(raw, arrays, ranks, W, K, mach, cfl, d)
+            res = run_reference_mpi(raw, arrays, ranks, W, K, mach, cfl, d, aoa=aoa)
         assert res["cells"] == cells and res["iterations"] == K, res
         tmax = res["seconds"]
         value = 5.0 * cells * K / tmax
@@ -590,7 +596,7 @@ def run_reference(args, rank, world):
 
         arrays = Mesh.from_raw(raw).arrays()
         m = po.Mesh(arrays)
-        fl = po.flow(mach, 0.0, 1.4, cfl)
+        fl = po.flow(mach, aoa, 1.4, cfl)
         s = po.freestream(m, fl)
         po.run(m, fl, s, 1)
         t = time.time()
