@@ -408,6 +408,8 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "parity": parity,
     }
     solver.close()
+    if rank == 0 and world == 1 and args.mode == "all" and args.precision == "fp64":
+        line["fp32_flux"] = fp32_flux_leg(arrays, flow, n_cells, n_faces, K, W, peak, local_rank)
     del arrays
     if rank == 0 and world == 1 and args.mode == "all":
         line["batch"] = batch_leg(local_rank, peak)
@@ -418,6 +420,55 @@ def run_ours(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp32_flux_leg(arrays, flow, n_cells: int, n_faces: int, K: int, W: int, peak: float, device: int) -> dict:
+    """The FP32_FLUX mode (fluxes, face states and time step in single precision; state, RK
+    accumulation and reductions in double) on the bench mesh: K RK5 iterations timed with CUDA events
+    after W untimed, the stage kernel's roofline fraction from its algorithmic bytes (104 + 24 f_c per
+    cell-stage), and its error against the FP64 path after the same W + K iterations from the
+    freestream (interior fields, velocity relative to the local speed; the wall force vector)."""
+    import dataclasses
+
+    import numpy as np
+    import torch
+
+    from euler3d_b200 import _lib
+    from euler3d_b200.solver import EulerSolver
+
+    stream = torch.cuda.Stream(device=device)
+    s32 = EulerSolver(arrays, dataclasses.replace(flow, precision=_lib.PREC_FP32_FLUX), stream=stream.cuda_stream)
+    s32.run(W, check_every=K)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st = s32.run(K, check_every=K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    assert st["iterations"] == K, st
+    g32, f32 = s32.get_state(), s32.coefficients()[0]
+    prof = s32.run(K, check_every=K, profile_stages=2)
+    stage_ms = prof["stage_ms"] / prof["stage_launches"]
+    variant = s32.info()["stage_variant"]
+    s32.close()
+    s64 = EulerSolver(arrays, dataclasses.replace(flow, precision=_lib.PREC_FP64), autotune=False)
+    s64.run(W + K, check_every=K)
+    g64, f64 = s64.get_state(), s64.coefficients()[0]
+    s64.close()
+    speed = np.sqrt(g64["u"][:n_cells] ** 2 + g64["v"][:n_cells] ** 2 + g64["w"][:n_cells] ** 2)
+    err = {}
+    for k in ("rho", "u", "v", "w", "p", "E", "H"):
+        scale = speed if k in ("u", "v", "w") else np.abs(g64[k][:n_cells])
+        err[k] = float(np.max(np.abs(g32[k][:n_cells] - g64[k][:n_cells]) / scale))
+    bpc = algorithmic_bytes_per_cell_stage(n_cells, n_faces, fp32=True)
+    return {"value": 5.0 * n_cells * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K, "steps": K, "warmup": W,
+            "stage_kernel": ["-", "-", "tile_kernel_f32<4>", "tile_ws_kernel<WS_F32>", "tile_kernel_f32<8>", "-", "-"][variant],
+            "avg_launch_ms": stage_ms, "bytes_per_cell_stage": bpc,
+            "achieved_GBs": bpc * n_cells / (stage_ms / 1e3) / 1e9,
+            "frac": bpc * n_cells / (stage_ms / 1e3) / 1e9 / peak,
+            "vs_fp64": {"iterations": W + K, "start": "freestream", "fields_max_rel": err,
+                        "force_rel": float(np.linalg.norm(np.subtract(f32, f64)) / max(np.linalg.norm(f64), 1e-300))}}
 
 
 def first_iteration_parity(solver, arrays, flow, oracle_state, n_cells, precision):
