@@ -63,3 +63,24 @@ def test_ranks_agree_with_one_rank(tmp_path):
     for k in (0, 4, 5):  # rho, p, E
         rel = np.max(np.abs(merged[k] - ref[k]) / np.abs(ref[k]))
         assert rel < 1e-5, (k, rel)  # measured 1e-7..5e-7 after 12 iterations
+
+
+@pytest.mark.parametrize("mesh,extra", [("c3", ["--n", "8"]), ("c1", [])])
+def test_bench_reference_arm_line(mesh, extra):
+    """`bench.py --impl reference` end to end on small cases: one JSON line with the contract's keys,
+    the reference kind, the rank count used and the same SAMPLING= as the GPU arm's timed runs."""
+    import json
+    import sys
+
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--ref-mesh", mesh,
+           "--ref-ranks", "2", "--steps", "2", "--warmup", "3"] + extra
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, start_new_session=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "RK-stage cell-updates/s" and line["value"] > 0
+    assert line["steps"] == 2 and line["warmup"] == 3 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] == 2
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["config"]["ranks"] == 2 and line["config"]["sampling"] == 1_000_000_000
+    assert line["config"]["cells"] == (8 ** 3 * 6 if mesh == "c3" else 64 * 32 * 2)
