@@ -11,7 +11,7 @@ void prepare_tile_f32(size_t smem_bytes, size_t ws_smem_bytes) {
 }
 
 void prepare_batch_f32(size_t smem_bytes, size_t ws_smem_bytes) {
-    raise_smem_limit((const void *)tile_batch_kernel_f32<7>, smem_bytes);
+    raise_smem_limit((const void *)tile_batch_kernel_f32<8>, smem_bytes);
     if (ws_smem_bytes) raise_smem_limit((const void *)tile_ws_batch_kernel<WS_F32>, ws_smem_bytes);
 }
 
@@ -22,7 +22,7 @@ void launch_batch_ws_f32(const BatchStage &bs, int grid, size_t smem_bytes, cuda
 
 // One stage of every member of a batch: `grid` blocks over the (member, tile) table.
 void launch_batch_f32(const BatchStage &bs, int grid, size_t smem_bytes, cudaStream_t s) {
-    tile_batch_kernel_f32<7><<<grid, kStageThreads, smem_bytes, s>>>(bs);
+    tile_batch_kernel_f32<8><<<grid, kStageThreads, smem_bytes, s>>>(bs);
 }
 
 // variant 2: face tiles with registers for four blocks/SM; 3: warp-specialised persistent face
