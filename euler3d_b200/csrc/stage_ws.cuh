@@ -27,6 +27,8 @@ namespace e3d {
 
 constexpr int kWsGroups = 5;
 constexpr int kWsThreads = 32 + kWsGroups * kTileCells;
+// Halo entries per producer lane loaded one item ahead (the first 32 x kWsPreHalo of a tile's halo).
+constexpr int kWsPreHalo = 8;
 // Bytes ahead of a batch buffer's tile data that hold the member's StageArgs.
 constexpr size_t kWsArgsSlot = (sizeof(StageArgs) + 127) & ~(size_t)127;
 static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is bulk-copied");
@@ -151,9 +153,92 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 0) {  // ------------------------------------------------ producer
+        // Everything an item's copies depend on -- its tile, sizes and source addresses, and this
+        // lane's first kWsPreHalo halo entries -- is loaded one item ahead, before the producer waits
+        // for the buffer of the item it issues now, so those global-memory round trips overlap that
+        // wait and the copies it issues, instead of running back to back once per tile.
+        struct Pre {
+            const StageArgs *a;
+            const char *st_src, *rec_src, *geo_src;
+            const unsigned short *ct_src;
+            const int *hrow;
+            const double *w0;
+            int tile, c0, nloc, nf, hs, w0_stride, lc, fc, mc;
+            bool skip;
+            int hidx[kWsPreHalo];
+        };
+        auto prepare = [&](int item, Pre &p) {
+            int tile;
+            const StageArgs &a = *item_args(item, tile);
+            p.a = &a;
+            p.tile = tile;
+            p.skip = BATCH && a.ctl->done;  // a stopped member: its arguments only
+            p.c0 = tile * T;
+            p.nloc = min(T, a.n_cells - p.c0);
+            p.lc = a.smem_cells, p.fc = a.smem_faces, p.mc = a.max_contrib;
+            const char *qsrc = F32 ? reinterpret_cast<const char *>(a.q32in) : reinterpret_cast<const char *>(a.qin);
+            p.st_src = qsrc;
+            p.nf = p.skip ? 0 : a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+            p.rec_src = p.skip ? nullptr : (F32 ? a.tile_rec32 + a.tile_rec32_off[tile] : a.tile_rec + a.tile_rec_off[tile]);
+            p.ct_src = a.tile_contrib + (size_t)tile * a.max_contrib * T;
+            p.w0 = a.w0;
+            p.w0_stride = a.w0_stride;
+            p.geo_src = F32 ? reinterpret_cast<const char *>(a.cgeo32) : reinterpret_cast<const char *>(a.cgeo);
+            // halo entries sit at a fixed stride per tile, padded with -1: no count needed to load them
+            p.hs = p.skip ? 0 : a.halo_stride;
+            p.hrow = a.tile_halo + (size_t)tile * a.halo_stride;
+#pragma unroll
+            for (int m = 0; m < kWsPreHalo; m++) {
+                const int i = lane + 32 * m;
+                p.hidx[m] = i < p.hs ? p.hrow[i] : -1;
+            }
+        };
+        auto issue = [&](const Pre &p, int bi) {
+            unsigned char *base = smem_raw + (size_t)bi * bb;
+            void *st, *rec;
+            unsigned short *ct;
+            if (F32) {
+                const Tile32 t = tile32_at(base + slot, p.lc, p.fc);
+                st = t.st, rec = t.rec, ct = t.ct;
+            } else {
+                const TileBuf t = tile_buf_at(base + slot, p.lc, p.fc, p.mc);
+                st = t.st, rec = t.rec, ct = t.ct;
+            }
+            if (lane == 0) {
+                const uint32_t b_ct = (uint32_t)p.mc * T * 2u;
+                const uint32_t tile_bytes =
+                    p.skip ? 0u : (uint32_t)p.nloc * kState + round16(kRec * (uint32_t)p.nf) + b_ct;
+                mbar_expect_tx(&full[bi], tile_bytes + (BATCH ? (uint32_t)sizeof(StageArgs) : 0u));
+                if (BATCH) bulk_g2s(base, p.a, (uint32_t)sizeof(StageArgs), &full[bi]);
+                if (!p.skip) {
+                    bulk_g2s(st, p.st_src + (size_t)kState * p.c0, (uint32_t)p.nloc * kState, &full[bi]);
+                    bulk_g2s(rec, p.rec_src, round16(kRec * (uint32_t)p.nf), &full[bi]);
+                    bulk_g2s(ct, p.ct_src, b_ct, &full[bi]);
+                    const uint32_t b_w0 = round16((uint32_t)p.nloc * 8u);
+                    for (int q = 0; q < 5; q++) bulk_prefetch_l2(p.w0 + (size_t)q * p.w0_stride + p.c0, b_w0);
+                    bulk_prefetch_l2(p.geo_src + (size_t)kGeo * p.c0, (uint32_t)p.nloc * kGeo);
+                }
+            }
+            if (!p.skip) {
+                char *hdst = static_cast<char *>(st) + (size_t)kState * p.nloc;
+#pragma unroll
+                for (int m = 0; m < kWsPreHalo; m++)
+                    if (p.hidx[m] >= 0)
+                        ws_halo_gather(hdst + (size_t)kState * (lane + 32 * m), p.st_src + (size_t)kState * p.hidx[m],
+                                       kState);
+                for (int i = lane + 32 * kWsPreHalo; i < p.hs; i += 32) {  // larger halos: the rest
+                    const int h = p.hrow[i];
+                    if (h >= 0) ws_halo_gather(hdst + (size_t)kState * i, p.st_src + (size_t)kState * h, kState);
+                }
+            }
+            cp_async_arrive_noinc(&full[bi]);  // every lane, with or without halo copies
+        };
         int issued = 0;  // items whose copies were issued
         bool stopped = false;
+        Pre cur{}, nxt{};
+        if ((int)blockIdx.x < n_items) prepare(blockIdx.x, cur);
         for (int k = 0, item = blockIdx.x; item < n_items; k++, item += G) {
+            if (item + G < n_items) prepare(item + G, nxt);  // in flight while this item waits
             int fill;
             const int bi = buffer_of(k, fill);
             if (fill >= 1) {  // the buffer's previous item (k - B) has been handed back
@@ -175,41 +260,9 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             }
-            unsigned char *base = smem_raw + (size_t)bi * bb;
-            int tile;
-            const StageArgs &a = *item_args(item, tile);
-            const bool skip = BATCH && a.ctl->done;  // a stopped member: its arguments only
-            void *st, *rec;
-            unsigned short *ct;
-            layout(base + slot, a, st, rec, ct);
-            const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-            const int nh = skip ? 0 : a.tile_halo_ptr[tile + 1] - a.tile_halo_ptr[tile];
-            const char *qsrc = F32 ? reinterpret_cast<const char *>(a.q32in) : reinterpret_cast<const char *>(a.qin);
-            if (lane == 0) {
-                const int nf = skip ? 0 : a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
-                const uint32_t b_ct = (uint32_t)a.max_contrib * T * 2u;
-                const uint32_t tile_bytes = skip ? 0u : (uint32_t)nloc * kState + round16(kRec * (uint32_t)nf) + b_ct;
-                mbar_expect_tx(&full[bi], tile_bytes + (BATCH ? (uint32_t)sizeof(StageArgs) : 0u));
-                if (BATCH) bulk_g2s(base, &a, (uint32_t)sizeof(StageArgs), &full[bi]);
-                if (!skip) {
-                    bulk_g2s(st, qsrc + (size_t)kState * c0, (uint32_t)nloc * kState, &full[bi]);
-                    const char *rsrc = F32 ? a.tile_rec32 + a.tile_rec32_off[tile] : a.tile_rec + a.tile_rec_off[tile];
-                    bulk_g2s(rec, rsrc, round16(kRec * (uint32_t)nf), &full[bi]);
-                    bulk_g2s(ct, a.tile_contrib + (size_t)tile * a.max_contrib * T, b_ct, &full[bi]);
-                    const uint32_t b_w0 = round16((uint32_t)nloc * 8u);
-                    for (int q = 0; q < 5; q++) bulk_prefetch_l2(a.w0 + (size_t)q * a.w0_stride + c0, b_w0);
-                    const char *gsrc = F32 ? reinterpret_cast<const char *>(a.cgeo32) : reinterpret_cast<const char *>(a.cgeo);
-                    bulk_prefetch_l2(gsrc + (size_t)kGeo * c0, (uint32_t)nloc * kGeo);
-                }
-            }
-            if (!skip) {
-                const int *hrow = a.tile_halo + (size_t)tile * a.halo_stride;
-                char *hdst = static_cast<char *>(st) + (size_t)kState * nloc;
-                for (int i = lane; i < nh; i += 32)
-                    ws_halo_gather(hdst + (size_t)kState * i, qsrc + (size_t)kState * hrow[i], kState);
-            }
-            cp_async_arrive_noinc(&full[bi]);  // every lane, with or without halo copies
+            issue(cur, bi);
             issued = k + 1;
+            cur = nxt;
         }
         // every copy issued must land before the block can leave (the consumers wait for them when
         // the walk completes; after a give-up they may not have)
