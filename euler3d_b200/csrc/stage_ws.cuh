@@ -43,9 +43,10 @@ __host__ __device__ __forceinline__ size_t ws_buffer_bytes(int prec, int LC, int
 }
 
 // Dynamic shared memory with B buffers of `stride` bytes: the buffers, a full and an empty mbarrier
-// per buffer, and four doubles per consumer group for its RMS partial.
+// per buffer, four doubles per consumer group for its RMS partial, and per buffer the face count of
+// the tile in it (an int, 16 bytes reserved).
 __host__ __device__ __forceinline__ size_t ws_smem_for(size_t stride, int buffers) {
-    return (size_t)buffers * stride + 16 * (size_t)buffers + 32 * (size_t)kWsGroups;
+    return (size_t)buffers * stride + 16 * (size_t)buffers + 32 * (size_t)kWsGroups + 16 * (size_t)buffers;
 }
 
 // Consumer groups for B buffers: one buffer per group up to kWsGroups groups, then more per group.
@@ -123,6 +124,9 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
     uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)B * bb);
     uint64_t *empty = full + B;
     double *gsum = reinterpret_cast<double *>(empty + B);  // [kWsGroups][4]
+    // face count of the tile in buffer b, written by the producer before its arrival on the buffer's
+    // full barrier (release) and read by the consumer after its wait on it (acquire)
+    int *meta = reinterpret_cast<int *>(gsum + 4 * kWsGroups);
     // the arguments (in global memory, or the kernel's own) of work item `item`, and its tile
     auto item_args = [&](int item, int &tile) -> const StageArgs * {
         if (!BATCH) {
@@ -205,6 +209,7 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
                 st = t.st, rec = t.rec, ct = t.ct;
             }
             if (lane == 0) {
+                meta[bi] = p.nf;
                 const uint32_t b_ct = (uint32_t)p.mc * T * 2u;
                 const uint32_t tile_bytes =
                     p.skip ? 0u : (uint32_t)p.nloc * kState + round16(kRec * (uint32_t)p.nf) + b_ct;
@@ -306,7 +311,7 @@ __device__ __forceinline__ void ws_body(const StageArgs &solo, const BatchStage 
         double r2 = 0.0;
         if (run) {
             const int c0 = tile * T, nloc = min(T, a.n_cells - c0);
-            const int nf = a.tile_face_ptr[tile + 1] - a.tile_face_ptr[tile];
+            const int nf = meta[bi];  // the producer's, instead of a global-memory round trip
             if (F32) {
                 const Tile32 b = tile32_at(base + slot, a.smem_cells, a.smem_faces);
                 tile_fluxes_f32(a, b, nf, c0, tid, T);
